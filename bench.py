@@ -1,0 +1,345 @@
+"""Benchmark of the sparse-grid interpolation hot path on B200.
+
+Workload (one GPU): one adaptive d=59 grid of 1,000,000 nodes grown by seeded
+random refinement (levels <= 7), TotalDof = 256, and 1,000,000 query points
+(first half uniform in [0,1]^59, second half N(0.5, 0.05^2) clipped to [0,1]).
+A step is one forward pass over all points.  The headline form is the batched
+FP32 + compensated kernel (SGI_FP32C); the plain FP64 kernel (bit-identical to
+the reference's gold path) is timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (one process per GPU under torchrun) every rank replicates the grid
+and evaluates its own 1M points (weak scaling, no collective on the data path).
+`--impl reference` times the reference's own CPU code (oracle/_ref, compiled
+from the reference sources) on the host cores over a bounded sample of points.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "hddm-solver-postprocessors_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+DIM, NNO, TD, NPTS = 59, 1_000_000, 256, 1_000_000
+GRID_SEED, POINT_SEED = 4, 40
+METRIC = "d=59 points/s: batched FP32+comp vs plain FP64 GPU @<=1e-7 rel err; %HBM peak"
+WORKLOAD = "C4: d=59 adaptive grid, 1M nodes (levels<=7), TotalDof=256, 1M points (half U[0,1], half N(0.5,0.05^2))"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_workload(npts=NPTS, seed_offset=0):
+    import hddm_b200 as H
+    t = time.time()
+    hg = H.HostGrid.adaptive(DIM, NNO, TD, seed=GRID_SEED)
+    X = H.gen_points(DIM, npts, kind=2, seed=POINT_SEED + seed_offset)
+    return hg, X, time.time() - t
+
+
+def alg_bytes(hg, info, npts, s_b):
+    """SURVEY 8(d) algorithmic bytes of one launch (each grid counted once)."""
+    idx, _ = hg.arrays()
+    i = idx[:, :DIM]
+    j = idx[:, DIM:]
+    nz = (i != 0) | (j != 0)
+    dims = np.broadcast_to(np.arange(DIM), i.shape)[nz].astype(np.int64)
+    keys = (dims << 32) | (i[nz].astype(np.int64) << 16) | j[nz].astype(np.int64)
+    szxps = int(np.unique(keys).size) + 1
+    return (npts * DIM * 8 + npts * TD * 8 + info.nno * TD * s_b + info.ncoarse * TD * 4
+            + 2 * info.nno * info.max_comps + 4 * szxps), szxps
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        for line in open(self.file.name):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                try:
+                    rows.append((float(f[1]), float(f[2]), f[5:9]))
+                except ValueError:
+                    pass
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(r[0] for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[2][k].lower().startswith("active")})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    import hddm_b200 as H
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    hg, X, t_gen = make_workload(seed_offset=rank)
+    t0 = time.time()
+    grid = H.Grid(hg, device=local, flags=H.BUILD_FP32)
+    t_upload = time.time() - t0
+    info = grid.info
+    x = torch.from_numpy(X).to(dev)
+    out32 = torch.empty((NPTS, TD), dtype=torch.float64, device=dev)
+    out64 = torch.empty((NPTS, TD), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(precision, out, steps, warmup):
+        for _ in range(warmup):
+            H.interpolate(grid, x, precision=precision, out=out, stream=stream)
+        barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record(stream)
+        for s in range(steps):
+            H.interpolate(grid, x, precision=precision, out=out, stream=stream)
+            ev[s + 1].record(stream)
+        barrier()
+        per = [ev[s].elapsed_time(ev[s + 1]) for s in range(steps)]
+        total = ev[0].elapsed_time(ev[steps])
+        kernels = H.last_launch().kernels
+        return total, per, kernels
+
+    # accuracy of the FP32C form against the FP64 form (bit-identical to gold), all points
+    H.interpolate(grid, x, precision=H.FP64, out=out64, stream=stream)
+    H.interpolate(grid, x, precision=H.FP32C, out=out32, stream=stream)
+    torch.cuda.synchronize(dev)
+    den = torch.maximum(out64.abs(), 1e-3 * out64.abs().amax(dim=1, keepdim=True))
+    perr = ((out32 - out64).abs() / den).amax(dim=1)
+    err_max, err_rms = float(perr.max()), float(perr.pow(2).mean().sqrt())
+    counts = H.active_count(grid, x[:65536], stream=stream).double()
+    mean_active = float(counts.mean())
+
+    with Clocks(local) as clk:
+        t32, per32, k32 = timed(H.FP32C, out32, args.steps, args.warmup)
+        t64, per64, k64 = timed(H.FP64, out64, args.steps, args.warmup)
+    clocks = clk.summary()
+
+    # end to end through the C ABI's host-pointer entry: pinned x in, pinned out back
+    xh = torch.from_numpy(X).pin_memory()
+    outh = torch.empty((NPTS, TD), dtype=torch.float64).pin_memory()
+    import ctypes
+    offs = np.array([0, NPTS], np.int64)
+    garr = (ctypes.c_void_p * 1)(grid.handle.value)
+
+    def e2e_once():
+        rc = H.lib.sgi_interpolate_host(1, garr, offs.ctypes.data, xh.data_ptr(), outh.data_ptr(), H.FP32C)
+        if rc:
+            raise H.SgiError(rc, H.lib.sgi_last_error().decode())
+
+    for _ in range(max(1, args.warmup)):
+        e2e_once()
+    barrier()
+    te = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_once()
+    barrier()
+    t_e2e = (time.perf_counter() - te) * 1e3
+
+    # max over ranks
+    def maxr(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t32, t64, t_e2e = maxr(t32), maxr(t64), maxr(t_e2e)
+    result = None
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        b32, szxps = alg_bytes(hg, info, NPTS, 4)
+        b64, _ = alg_bytes(hg, info, NPTS, 8)
+        ms32 = t32 / args.steps
+        ms64 = t64 / args.steps
+        ach = b32 / (ms32 * 1e-3) / 1e9
+        pts_s = NPTS * world / (ms32 * 1e-3)
+        pts64_s = NPTS * world / (ms64 * 1e-3)
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            traffic = json.load(open(tf)).get("fwd_f32c_bytes_per_launch")
+        result = {
+            "metric": METRIC,
+            "value": pts_s,
+            "unit": "points/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms32,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+comp (f64 in/out)",
+            "data": "synthetic: seeded adaptive grid and points (reference's large grids are not in its tree)",
+            "config": {"workload": WORKLOAD, "dim": DIM, "nno": info.nno, "TotalDof": TD, "points_per_gpu": NPTS,
+                       "max_comps": info.max_comps, "ncoarse": info.ncoarse, "szxps": szxps,
+                       "mean_active_nodes_per_point": mean_active,
+                       "l2": "inputs larger than L2 (x 472 MB, surplus 1 GB FP32 / 2 GB FP64)",
+                       "parallelism": f"replicated grid, points sharded, {world} GPU(s)"},
+            "points_x_outputs_per_s": pts_s * TD,
+            "fp64_form": {"points_per_s": pts64_s, "ms_per_step": ms64,
+                          "roofline_frac": b64 / (ms64 * 1e-3) / 1e9 / hbm},
+            "speedup_fp32c_vs_fp64_form": pts_s / pts64_s,
+            "fp32c_vs_gold_exact_fp64": {"max_rel_err": err_max, "rms_rel_err": err_rms, "points": NPTS},
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                         "peak_kind": f"{peak_kind} (burst copy)", "algorithmic_bytes_per_launch": b32,
+                         "traffic": traffic, "kernel": "fwd_f32c_kernel"},
+            "fma_work": {"mean_active_nodes": mean_active,
+                         "flops_per_launch": 2.0 * mean_active * TD * NPTS,
+                         "achieved_tflops": 2.0 * mean_active * TD * NPTS / (ms32 * 1e-3) / 1e12},
+            "e2e": {"value": NPTS * world / (t_e2e / args.steps * 1e-3), "unit": "points/s",
+                    "h2d_bytes_per_step": NPTS * DIM * 8, "d2h_bytes_per_step": NPTS * TD * 8},
+            "gpu_launches": args.steps * (k32 + k64),
+            "clocks": clocks,
+            "setup_s": {"generate": round(t_gen, 2), "layout_and_upload": round(t_upload, 2)},
+        }
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(hg, X, args.cpu_sample, args.cpu_variant)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+def cpu_baseline(hg, X, sample, variant):
+    """The reference's own CPU kernel (oracle/_ref) on a bounded sample of the
+    workload's points, one call per point, all host threads."""
+    import oracle as O
+    if not O.ref_available(variant):
+        return {"value": None, "unit": "points/s", "kind": "reference", "cores": 0,
+                "sample": f"oracle/_ref/libref_{variant}.so not built"}
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "grid.plt")
+        hg.write_plt(p)
+        t = time.time()
+        r = O.RefGrid(p, DIM, variant)
+        t_load = time.time() - t
+        cores = os.cpu_count() or 1
+        sub = np.ascontiguousarray(X[:sample // 2].tolist() + X[NPTS // 2:NPTS // 2 + sample - sample // 2].tolist())
+        r.interpolate(sub[:cores], nthreads=cores)
+        t = time.perf_counter()
+        r.interpolate(sub, nthreads=cores)
+        dt = time.perf_counter() - t
+    return {"value": len(sub) / dt, "unit": "points/s", "kind": "reference", "cores": cores,
+            "variant": variant, "load_s": round(t_load, 1),
+            "sample": f"{len(sub)} of the workload's points (half uniform, half clustered), "
+                      f"LinearBasis_{variant}_Generic_InterpolateArray per point, {cores} threads"}
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    import oracle as O
+    variant = args.cpu_variant
+    if not O.ref_available(variant):
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/libref_{variant}.so not built "
+                          "(needs the reference tree at build time)"}))
+        return
+    hg, X, _ = make_workload()
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "grid.plt")
+        hg.write_plt(p)
+        r = O.RefGrid(p, DIM, variant)
+        rng = np.random.default_rng(0)
+        times = []
+        for s in range(args.warmup + args.steps):
+            sub = X[rng.choice(NPTS, args.cpu_sample, replace=False)]
+            t = time.perf_counter()
+            r.interpolate(sub, nthreads=cores)
+            if s >= args.warmup:
+                times.append(time.perf_counter() - t)
+    ms = float(np.mean(times)) * 1e3
+    v = args.cpu_sample / (ms * 1e-3)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (same grid and points)",
+        "config": {"workload": WORKLOAD, "sample_points_per_step": args.cpu_sample},
+        "cpu_baseline": {"value": v, "unit": "points/s", "kind": "reference", "cores": cores,
+                         "sample": f"{args.cpu_sample} random points of the workload per step, "
+                                   f"LinearBasis_{variant}_Generic_InterpolateArray, {cores} threads"},
+        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=256)
+    ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

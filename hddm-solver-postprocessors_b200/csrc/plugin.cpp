@@ -1,0 +1,331 @@
+// The postprocessor plugin surface (include/sgi_plugin.h) over the C ABI.
+//
+// Error behaviour follows the reference plugin: a bad call prints the
+// reference's message through the parent's MPI_Process (include/process.h),
+// when the parent provides one, and aborts; without a parent it prints to
+// stderr and calls abort().
+#include <cuda_runtime_api.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "sgi.h"
+#include "sgi_plugin.h"
+
+// The parent's process facade (include/process.h:8-28), bound weakly.
+class MPI_Process
+{
+public :
+	void abort() __attribute__((weak));
+	void cout(const char* format, ...) __attribute__((weak));
+	void cerr(const char* format, ...) __attribute__((weak));
+};
+extern "C" int MPI_Process_get(MPI_Process**) __attribute__((weak));
+
+namespace {
+
+[[noreturn]] void die(const char* fmt, ...)
+{
+	char buf[2048];
+	va_list ap;
+	va_start(ap, fmt);
+	vsnprintf(buf, sizeof(buf), fmt, ap);
+	va_end(ap);
+	MPI_Process* process = nullptr;
+	if (MPI_Process_get && MPI_Process_get(&process) == 0 && process)
+	{
+		process->cerr("%s", buf);
+		process->abort();
+	}
+	fputs(buf, stderr);
+	fflush(stderr);
+	abort();
+}
+
+void say(const char* fmt, ...)
+{
+	if (!getenv("SGI_PLUGIN_VERBOSE")) return;
+	va_list ap;
+	va_start(ap, fmt);
+	vfprintf(stdout, fmt, ap);
+	va_end(ap);
+}
+
+// Globals behind Parameters' references (the reference keeps them global for
+// Fortran, LinearBasis/cpu/include/parameters.c:1-17).
+int g_priority = 0;
+int g_nagents = 0;
+double g_surplusCutoff = 0.0;
+bool g_surplusCutoffDefined = false;
+
+} // namespace
+
+namespace SGI_PLUGIN_NAMESPACE {
+
+class Device
+{
+public :
+	int index = 0;
+	int available = 1;
+	int warpSize = 32;
+	int cc = 0;
+	int sms = 0;
+};
+
+class DeviceProperties
+{
+public :
+	const Device* device;
+	explicit DeviceProperties(const Device* d) : device(d) { }
+	virtual const void* getSIMDVector() const { return nullptr; }
+	virtual ~DeviceProperties() { }
+};
+
+// Reads hddm-solver.cfg: "name value !comment" lines, the keys the CUDA
+// variant reads (LinearBasis/cuda/src/parameters.cpp:96-150).
+Parameters::Parameters(const std::string& targetSuffix, const std::string& configFile) :
+	priority(g_priority), nagents(g_nagents), surplusCutoff(g_surplusCutoff),
+	surplusCutoffDefined(g_surplusCutoffDefined)
+{
+	say("LOADING \"%s\" POSTPROCESSOR CONFIG (%s)\n", targetSuffix.c_str(), configFile.c_str());
+	bool havePriority = false, haveNagents = false, haveCutoff = false;
+	FILE* cfg = fopen(configFile.c_str(), "r");
+	if (!cfg) die("Cannot open config file \"%s\"\n", configFile.c_str());
+	char* line = nullptr;
+	size_t szline = 0;
+	while (getline(&line, &szline, cfg) != -1)
+	{
+		char* save = nullptr;
+		char* name = strtok_r(line, " \t\n", &save);
+		if (!name || name[0] == '!') continue;
+		char* value = strtok_r(nullptr, " \t\n", &save);
+		if (!value || value[0] == '!')
+		{
+			std::string n(name);
+			fclose(cfg);
+			free(line);
+			die("Missing \"%s\" parameter value\n", n.c_str());
+		}
+		if (!strcmp(name, "priorityCUDA")) { priority = atoi(value); havePriority = true; }
+		else if (!strcmp(name, "n_agents") || !strcmp(name, "nagents")) { nagents = atoi(value); haveNagents = true; }
+		else if (!strcmp(name, "surplusCutoff")) { surplusCutoff = atof(value); haveCutoff = true; }
+	}
+	free(line);
+	fclose(cfg);
+	surplusCutoffDefined = haveCutoff;
+	if (!havePriority) die("Required parameter \"%s\" is undefined\n", "priority");
+	if (!haveNagents) die("Required parameter \"%s\" is undefined\n", "nagents");
+}
+
+// All states of one multistate set; each state a device grid.
+class Data
+{
+public :
+	int nstates, dim = 0, TotalDof = 0;
+	std::vector<sgi_grid_t> grids;
+	std::vector<bool> loaded;
+
+	explicit Data(int n) : nstates(n), grids(n, nullptr), loaded(n, false) { }
+
+	// LinearBasis/cuda/src/Data.cu:348-949 (via gold/src/Data.cpp:322-436 checks)
+	virtual void load(const char* filename, int istate)
+	{
+		const Parameters& params = Interpolator::getInstance()->getParameters();
+		if (istate < 0 || istate >= nstates) die("State %d index out of range 0 .. %d\n", istate, nstates - 1);
+		if (loaded[istate]) die("State %d data is already loaded\n", istate);
+		sgi_host_grid_t hg = nullptr;
+		int rc = sgi_host_grid_read_plt(filename, params.nagents, &hg);
+		if (rc) die("%s\n", sgi_last_error());
+		int d = 0, nno = 0, td = 0;
+		sgi_host_grid_view(hg, &d, &nno, &td, nullptr, nullptr);
+		bool first = true;
+		for (int s = 0; s < nstates; s++) if (loaded[s]) first = false;
+		if (first) { dim = d; TotalDof = td; }
+		else
+		{
+			if (d != dim) { sgi_host_grid_free(hg); die("File \"%s\" # of dimensions (%d) mismatches another state (%d)\n", filename, d, dim); }
+			if (td != TotalDof) { sgi_host_grid_free(hg); die("File \"%s\" TotalDof (%d) mismatches another state (%d)\n", filename, td, TotalDof); }
+		}
+		int dev = 0;
+		cudaGetDevice(&dev);
+		sgi_grid_t g = nullptr;
+		rc = sgi_grid_create(hg, dev, 0u, &g);
+		sgi_host_grid_free(hg);
+		if (rc) die("%s\n", sgi_last_error());
+		grids[istate] = g;
+		loaded[istate] = true;
+	}
+
+	virtual void clear()
+	{
+		for (int s = 0; s < nstates; s++)
+		{
+			if (grids[s]) sgi_grid_destroy(grids[s]);
+			grids[s] = nullptr;
+			loaded[s] = false;
+		}
+	}
+
+	virtual ~Data() { clear(); }
+};
+
+namespace {
+std::unique_ptr<Interpolator> interp;
+std::mutex interp_mtx;
+}
+
+const Parameters& Interpolator::getParameters() const { return params; }
+
+Interpolator::Interpolator(const std::string& targetSuffix, const std::string& configFile) :
+	jit(false), params(targetSuffix, configFile) { }
+
+Interpolator::~Interpolator() { }
+
+Interpolator* Interpolator::getInstance()
+{
+	std::lock_guard<std::mutex> lk(interp_mtx);
+	if (!interp) interp.reset(new Interpolator("b200"));
+	return interp.get();
+}
+
+static void check_dof(const Data* data, int DofPerNode)
+{
+	if (DofPerNode != data->TotalDof)
+		die("Requested DofPerNode (%d) mismatches actual data TotalDof (%d)\n", DofPerNode, data->TotalDof);
+}
+
+void Interpolator::interpolate(Device* device, Data* data, const int istate, const real* x,
+	const int DofPerNode, real* value)
+{
+	(void)device;
+	check_dof(data, DofPerNode);
+	if (istate < 0 || istate >= data->nstates || !data->loaded[istate])
+		die("State %d is not loaded\n", istate);
+	const long long off[2] = { 0, 1 };
+	int rc = sgi_interpolate_host(1, &data->grids[istate], off, x, value, SGI_FP64);
+	if (rc) die("%s\n", sgi_last_error());
+}
+
+void Interpolator::interpolate(Device* device, Data* data, const real** x, const int DofPerNode, real** value)
+{
+	(void)device;
+	check_dof(data, DofPerNode);
+	const int n = data->nstates;
+	for (int s = 0; s < n; s++) if (!data->loaded[s]) die("State %d is not loaded\n", s);
+	std::vector<long long> off(n + 1);
+	for (int s = 0; s <= n; s++) off[s] = s;
+	std::vector<double> xb((size_t)n * data->dim), vb((size_t)n * data->TotalDof);
+	for (int s = 0; s < n; s++) memcpy(&xb[(size_t)s * data->dim], x[s], sizeof(double) * data->dim);
+	int rc = sgi_interpolate_host(n, data->grids.data(), off.data(), xb.data(), vb.data(), SGI_FP64);
+	if (rc) die("%s\n", sgi_last_error());
+	for (int s = 0; s < n; s++) memcpy(value[s], &vb[(size_t)s * data->TotalDof], sizeof(double) * data->TotalDof);
+}
+
+} // namespace SGI_PLUGIN_NAMESPACE
+
+using namespace SGI_PLUGIN_NAMESPACE;
+
+namespace {
+
+struct Devices
+{
+	std::vector<Device> devs;
+	std::vector<std::unique_ptr<DeviceProperties>> props;
+	std::vector<DeviceProperties*> props_raw;
+	std::mutex mtx;
+	Devices()
+	{
+		const int n = sgi_device_count();
+		devs.resize(n);
+		for (int i = 0; i < n; i++)
+		{
+			cudaDeviceProp p;
+			if (cudaGetDeviceProperties(&p, i) == cudaSuccess)
+			{
+				devs[i].warpSize = p.warpSize;
+				devs[i].cc = p.major * 10 + p.minor;
+				devs[i].sms = p.multiProcessorCount;
+			}
+			devs[i].index = i;
+		}
+		for (int i = 0; i < n; i++)
+		{
+			props.emplace_back(new DeviceProperties(&devs[i]));
+			props_raw.push_back(props.back().get());
+		}
+	}
+};
+
+Devices& devices()
+{
+	static Devices d;
+	return d;
+}
+
+} // namespace
+
+extern "C" Interpolator* getInterpolator() { return Interpolator::getInstance(); }
+
+extern "C" Data* getData(int nstates) { return new Data(nstates); }
+
+extern "C" bool isSupported() { return sgi_device_count() > 0; }
+
+extern "C" int getPriority() { return Interpolator::getInstance()->getParameters().priority; }
+
+extern "C" void resetInterpolator()
+{
+	std::lock_guard<std::mutex> lk(interp_mtx);
+	interp = nullptr;
+}
+
+extern "C" Device* tryAcquireDevice()
+{
+	Devices& d = devices();
+	std::lock_guard<std::mutex> lk(d.mtx);
+	for (auto& dev : d.devs)
+		if (dev.available) { dev.available = 0; return &dev; }
+	return nullptr;
+}
+
+extern "C" void releaseDevice(Device* device)
+{
+	if (!device) return;
+	Devices& d = devices();
+	std::lock_guard<std::mutex> lk(d.mtx);
+	device->available++;
+}
+
+extern "C" void getDeviceProperties(DeviceProperties*** result, size_t* szresult)
+{
+	Devices& d = devices();
+	*result = d.props_raw.empty() ? nullptr : d.props_raw.data();
+	*szresult = d.props_raw.size();
+}
+
+extern "C" int sgi_plugin_data_load(Data* data, const char* filename, int istate)
+{
+	data->load(filename, istate);
+	return 0;
+}
+
+extern "C" void sgi_plugin_interpolate(Device* device, Data* data, int istate, const double* x,
+	int DofPerNode, double* value)
+{
+	getInterpolator()->interpolate(device, data, istate, x, DofPerNode, value);
+}
+
+extern "C" void sgi_plugin_interpolate_multistate(Device* device, Data* data, const double** x,
+	int DofPerNode, double** value)
+{
+	getInterpolator()->interpolate(device, data, x, DofPerNode, value);
+}
+
+extern "C" void sgi_plugin_data_free(Data* data) { delete data; }
+
+extern "C" int sgi_plugin_device_index(const Device* device) { return device ? device->index : -1; }

@@ -1,0 +1,888 @@
+// Device layer of the B200 sparse-grid interpolator (sm_100a).
+//
+// Grid layout (built by sgi::build_layout): nodes in grid order, each with a
+// 16-byte record {skip, comp_ptr, ncomp|flags|delta dim, delta (i, j)} and a
+// CSR list of its non-constant components (dim, i, j) in dimension order.
+// Every node's support lies inside its tree parent's support, and a node's
+// subtree is the index range [n, skip[n]).
+//
+// Forward kernel: one warp per query point, points pulled from a device work
+// counter.  The warp walks the nodes in windows of 32 consecutive indices:
+//   * lane k checks node n0+k against the point with one hat evaluation (the
+//     component in which it differs from its parent);
+//   * an inclusive max-scan of the skip pointers of failing nodes marks every
+//     node inside a failing node's subtree as pruned;
+//   * surviving nodes ("hits") get their weight, the product of all their
+//     hats in dimension order, from their own lane;
+//   * hits are accumulated in index order: all lanes read the node's surplus
+//     row (coalesced) and update the TotalDof accumulators they own;
+//   * the next window starts after the window or after the largest pruned
+//     subtree, whichever is further.
+// With nodes in file order, the FP64 form performs the reference gold kernel's
+// operations in its order (LinearBasis/gold/src/InterpolateArray.cpp:26-41):
+// the same multiplies for the weight and the same multiply-then-add sequence per
+// output, so its results are bit-identical to gold's.
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "sgi_internal.h"
+
+using namespace sgi;
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int MAXG = 48;       // grids per launch (kernel parameter space)
+constexpr int BLOCK = 256;     // threads per block: 8 warps
+constexpr int WARPS = BLOCK / 32;
+constexpr int RMAX = 8;        // accumulator slots per lane: 256 outputs per pass
+
+struct GridDesc
+{
+	const uint4* rec;
+	const uint2* comps;
+	const double* s64;
+	const float* s32;
+	const float* s32lo;
+	const uint32_t* lo_index;
+	long long pt_begin;
+	int nno;
+	int ld;
+};
+
+struct FwdArgs
+{
+	GridDesc g[MAXG];
+	const double* x;
+	double* out;
+	unsigned long long* counter;
+	long long npts;
+	int ngrids, dim, TD, o_begin;
+};
+
+__device__ __forceinline__ double hat(double x, uint32_t ij)
+{
+	// 1 - |x*i - j| with the gold macro's rounding (LinearBasis/include/LinearBasis.h:50)
+	return __dsub_rn(1.0, fabs(__dsub_rn(__dmul_rn(x, (double)(ij & 0xffffu)), (double)(ij >> 16))));
+}
+
+__device__ __forceinline__ int find_grid(const FwdArgs& a, long long p)
+{
+	int gi = 0;
+	while (gi + 1 < a.ngrids && a.g[gi + 1].pt_begin <= p) gi++;
+	return gi;
+}
+
+// Walks one grid for the point whose coordinates are in xs (shared memory).
+// Calls on_hits(mask, n0, w, rec) per window; bits of mask are hit lanes,
+// lane k's w is the weight of node n0+k and rec its record.
+template <class OnHits>
+__device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, OnHits&& on_hits)
+{
+	int n0 = 0;
+	const int nno = G.nno;
+	while (n0 < nno)
+	{
+		const int idx = n0 + lane;
+		const bool valid = idx < nno;
+		uint4 r = make_uint4(0u, 0u, 0u, 0u);
+		if (valid) r = __ldg(G.rec + idx);
+		const uint32_t ncomp = r.z & 0xffu;
+		bool act = false;
+		if (valid)
+		{
+			if (r.z & NODE_DEAD) act = false;
+			else if (r.z & NODE_ALWAYS) act = true;
+			else if (r.z & NODE_MULTI)
+			{
+				act = true;
+				for (uint32_t c = 0; c < ncomp && act; c++)
+				{
+					const uint2 cp = __ldg(G.comps + r.y + c);
+					act = hat(xs[cp.x], cp.y) > 0.0;
+				}
+			}
+			else act = hat(xs[r.z >> 16], r.w) > 0.0;
+		}
+		const unsigned cover = (valid && !act) ? r.x : 0u;
+		unsigned inc = cover;
+#pragma unroll
+		for (int off = 1; off < 32; off <<= 1)
+		{
+			const unsigned v = __shfl_up_sync(FULL, inc, off);
+			if (lane >= off) inc = max(inc, v);
+		}
+		unsigned exc = __shfl_up_sync(FULL, inc, 1);
+		if (lane == 0) exc = 0u;
+		const bool hit = act && exc <= (unsigned)idx;
+		const unsigned mask = __ballot_sync(FULL, hit);
+		double w = 0.0;
+		if (hit)
+		{
+			w = 1.0;
+			for (uint32_t c = 0; c < ncomp; c++)
+			{
+				const uint2 cp = __ldg(G.comps + r.y + c);
+				w = __dmul_rn(w, hat(xs[cp.x], cp.y));
+			}
+		}
+		if (mask) on_hits(mask, n0, w, r);
+		const unsigned last = __shfl_sync(FULL, inc, 31);
+		n0 = max(n0 + 32, (int)last);
+	}
+}
+
+// Loads point p into the warp's shared slot; returns false (after writing NaN
+// outputs, as the gold kernel produces for a non-finite coordinate) if any
+// coordinate is not finite.
+__device__ __forceinline__ bool load_point(const FwdArgs& a, long long p, double* xs, int lane)
+{
+	bool finite = true;
+	for (int k = lane; k < a.dim; k += 32)
+	{
+		const double v = a.x[(size_t)p * a.dim + k];
+		xs[k] = v;
+		finite &= isfinite(v);
+	}
+	__syncwarp();
+	return __all_sync(FULL, finite);
+}
+
+template <int R>
+__global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ FwdArgs a)
+{
+	extern __shared__ double smem[];
+	const int lane = threadIdx.x & 31;
+	double* xs = smem + (threadIdx.x >> 5) * a.dim;
+	for (;;)
+	{
+		long long p = 0;
+		if (lane == 0) p = (long long)atomicAdd(a.counter, 1ull);
+		p = __shfl_sync(FULL, p, 0);
+		if (p >= a.npts) break;
+		const GridDesc& G = a.g[find_grid(a, p)];
+		double acc[R];
+#pragma unroll
+		for (int r = 0; r < R; r++) acc[r] = 0.0;
+		const bool ok = load_point(a, p, xs, lane);
+		if (ok)
+		{
+			traverse(G, xs, lane, [&](unsigned mask, int n0, double w, const uint4&)
+			{
+				while (mask)
+				{
+					const int k = __ffs(mask) - 1;
+					mask &= mask - 1;
+					const double wk = __shfl_sync(FULL, w, k);
+					const double* row = G.s64 + (size_t)(n0 + k) * G.ld + a.o_begin;
+#pragma unroll
+					for (int r = 0; r < R; r++)
+					{
+						const int o = lane + 32 * r;
+						if (a.o_begin + o < G.ld) acc[r] = __dadd_rn(acc[r], __dmul_rn(wk, __ldg(row + o)));
+					}
+				}
+			});
+		}
+		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
+#pragma unroll
+		for (int r = 0; r < R; r++)
+		{
+			const int o = lane + 32 * r;
+			if (a.o_begin + o < a.TD) dst[o] = ok ? acc[r] : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0);
+		}
+		__syncwarp();
+	}
+}
+
+// FP32 + compensated form.  Per output: a double-float accumulator (hi, lo)
+// for coarse rows, whose terms are formed from the hi/lo splits of weight and
+// surplus with an exact FMA product error, added with TwoSum; a plain FP32
+// FMA accumulator for the other rows; the three parts are summed in FP64 at
+// the end.
+template <int R>
+__global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__ FwdArgs a)
+{
+	extern __shared__ double smem[];
+	const int lane = threadIdx.x & 31;
+	double* xs = smem + (threadIdx.x >> 5) * a.dim;
+	for (;;)
+	{
+		long long p = 0;
+		if (lane == 0) p = (long long)atomicAdd(a.counter, 1ull);
+		p = __shfl_sync(FULL, p, 0);
+		if (p >= a.npts) break;
+		const GridDesc& G = a.g[find_grid(a, p)];
+		float ch[R], cl[R], fa[R];
+#pragma unroll
+		for (int r = 0; r < R; r++) { ch[r] = 0.f; cl[r] = 0.f; fa[r] = 0.f; }
+		const bool ok = load_point(a, p, xs, lane);
+		if (ok)
+		{
+			traverse(G, xs, lane, [&](unsigned mask, int n0, double w, const uint4& rec)
+			{
+				uint32_t lo = 0u;
+				if ((mask >> lane) & 1u)
+					if (rec.z & NODE_COARSE) lo = __ldg(G.lo_index + n0 + lane);
+				while (mask)
+				{
+					const int k = __ffs(mask) - 1;
+					mask &= mask - 1;
+					const double wk = __shfl_sync(FULL, w, k);
+					const uint32_t zk = __shfl_sync(FULL, rec.z, k);
+					const uint32_t lok = __shfl_sync(FULL, lo, k);
+					const float whi = __double2float_rn(wk);
+					const float* row = G.s32 + (size_t)(n0 + k) * G.ld + a.o_begin;
+					if (zk & NODE_COARSE)
+					{
+						const float wlo = __double2float_rn(wk - (double)whi);
+						const float* rlo = G.s32lo + (size_t)lok * G.ld + a.o_begin;
+#pragma unroll
+						for (int r = 0; r < R; r++)
+						{
+							const int o = lane + 32 * r;
+							if (a.o_begin + o < G.ld)
+							{
+								const float shi = __ldg(row + o), slo = __ldg(rlo + o);
+								const float pr = __fmul_rn(whi, shi);
+								const float pe = __fmaf_rn(whi, shi, -pr);
+								const float tl = __fmaf_rn(whi, slo, __fmaf_rn(wlo, shi, pe));
+								const float s = __fadd_rn(ch[r], pr);
+								const float bp = __fsub_rn(s, ch[r]);
+								const float e = __fadd_rn(__fsub_rn(ch[r], __fsub_rn(s, bp)), __fsub_rn(pr, bp));
+								ch[r] = s;
+								cl[r] = __fadd_rn(cl[r], __fadd_rn(e, tl));
+							}
+						}
+					}
+					else
+					{
+#pragma unroll
+						for (int r = 0; r < R; r++)
+						{
+							const int o = lane + 32 * r;
+							if (a.o_begin + o < G.ld) fa[r] = __fmaf_rn(whi, __ldg(row + o), fa[r]);
+						}
+					}
+				}
+			});
+		}
+		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
+#pragma unroll
+		for (int r = 0; r < R; r++)
+		{
+			const int o = lane + 32 * r;
+			if (a.o_begin + o < a.TD)
+				dst[o] = ok ? ((double)ch[r] + (double)cl[r]) + (double)fa[r]
+				            : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0);
+		}
+		__syncwarp();
+	}
+}
+
+// Active-node count per point (single grid).
+__global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ FwdArgs a, long long* counts)
+{
+	extern __shared__ double smem[];
+	const int lane = threadIdx.x & 31;
+	double* xs = smem + (threadIdx.x >> 5) * a.dim;
+	for (;;)
+	{
+		long long p = 0;
+		if (lane == 0) p = (long long)atomicAdd(a.counter, 1ull);
+		p = __shfl_sync(FULL, p, 0);
+		if (p >= a.npts) break;
+		const GridDesc& G = a.g[find_grid(a, p)];
+		long long cnt = 0;
+		if (load_point(a, p, xs, lane))
+			traverse(G, xs, lane, [&](unsigned mask, int, double, const uint4&) { cnt += __popc(mask); });
+		if (lane == 0) counts[p] = cnt;
+		__syncwarp();
+	}
+}
+
+// ------------------------------------------------------------------ backward
+//
+// dL/dx: per point (one warp), for every active node n the scalar
+// cs = sum_o gout[p,o] * s[n,o] (warp reduction), then for each component c of
+// n, dw/dx_{dim c} = (prod of the other hats) * slope_c, slope = -i sign(x i - j).
+// dL/dsurplus: pairs (node, point, weight) are written at per-point offsets
+// (exclusive scan of the active counts: no atomics), stably radix-sorted by
+// node, and each node's segment is reduced by one warp in point order.
+
+struct BwdArgs
+{
+	GridDesc G;
+	const double* x;
+	const double* gout;
+	double* gx;
+	const long long* pair_off;   // npts + 1, or null
+	uint32_t* pair_node;
+	uint32_t* pair_point;
+	double* pair_w;
+	unsigned long long* counter;
+	long long npts;
+	int dim, TD;
+};
+
+template <int R>
+__global__ void __launch_bounds__(BLOCK) bwd_points_kernel(const __grid_constant__ BwdArgs a)
+{
+	extern __shared__ double smem[];
+	const int lane = threadIdx.x & 31;
+	double* xs = smem + (threadIdx.x >> 5) * 2 * a.dim;
+	double* gxs = xs + a.dim;
+	const GridDesc& G = a.G;
+	for (;;)
+	{
+		long long p = 0;
+		if (lane == 0) p = (long long)atomicAdd(a.counter, 1ull);
+		p = __shfl_sync(FULL, p, 0);
+		if (p >= a.npts) break;
+		for (int k = lane; k < a.dim; k += 32) { xs[k] = a.x[(size_t)p * a.dim + k]; gxs[k] = 0.0; }
+		double g[R];
+#pragma unroll
+		for (int r = 0; r < R; r++)
+		{
+			const int o = lane + 32 * r;
+			g[r] = o < a.TD ? a.gout[(size_t)p * a.TD + o] : 0.0;
+		}
+		__syncwarp();
+		long long woff = a.pair_off ? a.pair_off[p] : 0;
+		traverse(G, xs, lane, [&](unsigned mask, int n0, double w, const uint4& rec)
+		{
+			if (a.pair_off)
+			{
+				const int rank = __popc(mask & ((1u << lane) - 1u));
+				if ((mask >> lane) & 1u)
+				{
+					a.pair_node[woff + rank] = (uint32_t)(n0 + lane);
+					a.pair_point[woff + rank] = (uint32_t)p;
+					a.pair_w[woff + rank] = w;
+				}
+				woff += __popc(mask);
+			}
+			if (!a.gx) return;
+			while (mask)
+			{
+				const int k = __ffs(mask) - 1;
+				mask &= mask - 1;
+				const double* row = G.s64 + (size_t)(n0 + k) * G.ld;
+				double cs = 0.0;
+#pragma unroll
+				for (int r = 0; r < R; r++)
+				{
+					const int o = lane + 32 * r;
+					if (o < a.TD) cs = fma(g[r], __ldg(row + o), cs);
+				}
+#pragma unroll
+				for (int off = 16; off > 0; off >>= 1) cs += __shfl_xor_sync(FULL, cs, off);
+				const uint32_t cptr = __shfl_sync(FULL, rec.y, k);
+				const uint32_t ncomp = __shfl_sync(FULL, rec.z, k) & 0xffu;
+				for (uint32_t c = lane; c < ncomp; c += 32)
+				{
+					const uint2 cp = __ldg(G.comps + cptr + c);
+					double others = 1.0;
+					for (uint32_t q = 0; q < ncomp; q++)
+						if (q != c)
+						{
+							const uint2 cq = __ldg(G.comps + cptr + q);
+							others *= hat(xs[cq.x], cq.y);
+						}
+					const double t = xs[cp.x] * (double)(cp.y & 0xffffu) - (double)(cp.y >> 16);
+					const double slope = t > 0.0 ? -(double)(cp.y & 0xffffu) : (t < 0.0 ? (double)(cp.y & 0xffffu) : 0.0);
+					gxs[cp.x] += cs * others * slope;
+				}
+				__syncwarp();
+			}
+		});
+		if (a.gx)
+			for (int k = lane; k < a.dim; k += 32) a.gx[(size_t)p * a.dim + k] = gxs[k];
+		__syncwarp();
+	}
+}
+
+// One warp per node: dL/dsurplus[n, :] = sum over its pairs of w * gout[point, :].
+template <int R>
+__global__ void __launch_bounds__(BLOCK) bwd_surplus_kernel(const uint32_t* __restrict__ sorted_node,
+	const uint32_t* __restrict__ order, const uint32_t* __restrict__ pair_point, const double* __restrict__ pair_w,
+	long long npairs, const double* __restrict__ gout, double* __restrict__ gs, int nno, int TD)
+{
+	const int lane = threadIdx.x & 31;
+	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+	for (long long n = warp; n < nno; n += nwarps)
+	{
+		// segment [lo, hi) of node n in the sorted keys
+		long long lo = 0, hi = npairs;
+		while (lo < hi) { long long m = (lo + hi) >> 1; if (sorted_node[m] < (uint32_t)n) lo = m + 1; else hi = m; }
+		long long e = lo, h2 = npairs;
+		while (e < h2) { long long m = (e + h2) >> 1; if (sorted_node[m] <= (uint32_t)n) e = m + 1; else h2 = m; }
+		double acc[R];
+#pragma unroll
+		for (int r = 0; r < R; r++) acc[r] = 0.0;
+		for (long long q = lo; q < e; q++)
+		{
+			const uint32_t pi = order[q];
+			const double w = pair_w[pi];
+			const double* grow = gout + (size_t)pair_point[pi] * TD;
+#pragma unroll
+			for (int r = 0; r < R; r++)
+			{
+				const int o = lane + 32 * r;
+				if (o < TD) acc[r] = fma(w, grow[o], acc[r]);
+			}
+		}
+#pragma unroll
+		for (int r = 0; r < R; r++)
+		{
+			const int o = lane + 32 * r;
+			if (o < TD) gs[(size_t)n * TD + o] = acc[r];
+		}
+	}
+}
+
+__global__ void iota_kernel(uint32_t* v, long long n)
+{
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		v[i] = (uint32_t)i;
+}
+
+// ------------------------------------------------------------ host helpers
+
+thread_local sgi_launch_stats g_stats{};
+
+#define CUDA_TRY(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
+	return fail(SGI_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); } while (0)
+
+// Per-device workspace: a ring of work counters (one per launch; a counter is
+// reused after 65536 later launches on the device) and staging buffers for
+// the host-pointer entry point.
+struct DeviceWork
+{
+	std::mutex mtx;
+	unsigned long long* counters = nullptr;
+	std::atomic<unsigned> next{0};
+	int sms = 0;
+	// host-pointer staging
+	double* dx = nullptr; size_t dx_bytes = 0;
+	double* dout = nullptr; size_t dout_bytes = 0;
+	cudaStream_t stream = nullptr;
+};
+constexpr unsigned NCOUNTERS = 1u << 16;
+
+std::mutex g_work_mtx;
+std::vector<DeviceWork*> g_work;
+
+int device_work(int dev, DeviceWork** out)
+{
+	std::lock_guard<std::mutex> lk(g_work_mtx);
+	if ((int)g_work.size() <= dev) g_work.resize(dev + 1, nullptr);
+	if (!g_work[dev])
+	{
+		DeviceWork* w = new DeviceWork;
+		CUDA_TRY(cudaMalloc(&w->counters, sizeof(unsigned long long) * NCOUNTERS));
+		CUDA_TRY(cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, dev));
+		g_work[dev] = w;
+	}
+	*out = g_work[dev];
+	return SGI_OK;
+}
+
+int pick_R(int cols)
+{
+	if (cols <= 32) return 1;
+	if (cols <= 64) return 2;
+	if (cols <= 128) return 4;
+	return 8;
+}
+
+template <class K>
+int occupancy_grid(K kernel, size_t smem, int sms, int* blocks)
+{
+	int per_sm = 0;
+	CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BLOCK, smem));
+	if (per_sm < 1) return fail(SGI_E_CUDA, "kernel does not fit on an SM (smem %zu)", smem);
+	*blocks = per_sm * sms;
+	return SGI_OK;
+}
+
+} // namespace
+
+// ------------------------------------------------------------- grid object
+
+struct sgi_grid
+{
+	int device = 0;
+	int dim = 0, nno = 0, TD = 0, ld = 0;
+	uint4* rec = nullptr;
+	uint2* comps = nullptr;
+	double* s64 = nullptr;
+	float* s32 = nullptr;
+	float* s32lo = nullptr;
+	uint32_t* lo_index = nullptr;
+	sgi_grid_info info{};
+};
+
+namespace {
+
+void free_grid(sgi_grid* g)
+{
+	if (!g) return;
+	int prev = 0;
+	cudaGetDevice(&prev);
+	cudaSetDevice(g->device);
+	cudaFree(g->rec); cudaFree(g->comps); cudaFree(g->s64); cudaFree(g->s32); cudaFree(g->s32lo); cudaFree(g->lo_index);
+	cudaSetDevice(prev);
+	delete g;
+}
+
+GridDesc desc_of(const sgi_grid* g, long long pt_begin)
+{
+	GridDesc d;
+	d.rec = g->rec; d.comps = g->comps; d.s64 = g->s64; d.s32 = g->s32; d.s32lo = g->s32lo;
+	d.lo_index = g->lo_index; d.pt_begin = pt_begin; d.nno = g->nno; d.ld = g->ld;
+	return d;
+}
+
+struct DeviceGuard
+{
+	int prev = -1;
+	explicit DeviceGuard(int dev) { cudaGetDevice(&prev); cudaSetDevice(dev); }
+	~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+} // namespace
+
+extern "C" int sgi_device_count(void)
+{
+	int n = 0;
+	if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+	return n;
+}
+
+extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, sgi_grid_t* out)
+{
+	clear_error();
+	if (!hg || !out) return fail(SGI_E_INVALID, "null argument");
+	*out = nullptr;
+	const HostGrid& g = hg->g;
+	if (g.nno > 0x7fffffff - 64) return fail(SGI_E_RANGE, "too many nodes");
+	int ndev = sgi_device_count();
+	if (ndev == 0) return fail(SGI_E_NODEVICE, "no CUDA device");
+	if (device < 0 || device >= ndev) return fail(SGI_E_INVALID, "device %d out of range (%d devices)", device, ndev);
+	DeviceLayout L;
+	int rc = build_layout(g, L);
+	if (rc) return rc;
+	DeviceGuard guard(device);
+	sgi_grid* d = new sgi_grid;
+	d->device = device; d->dim = g.dim; d->nno = g.nno; d->TD = g.TotalDof;
+	d->ld = (g.TotalDof + 31) / 32 * 32;
+	const size_t nrow = (size_t)std::max(g.nno, 1);
+	long long bytes = 0;
+	auto upload = [&](void** dst, const void* src, size_t n) -> int
+	{
+		cudaError_t e = cudaMalloc(dst, std::max<size_t>(n, 16));
+		if (e != cudaSuccess) return fail(SGI_E_NOMEM, "cudaMalloc(%zu) failed: %s", n, cudaGetErrorString(e));
+		bytes += (long long)n;
+		if (n && src)
+		{
+			e = cudaMemcpy(*dst, src, n, cudaMemcpyHostToDevice);
+			if (e != cudaSuccess) return fail(SGI_E_CUDA, "cudaMemcpy failed: %s", cudaGetErrorString(e));
+		}
+		return SGI_OK;
+	};
+	rc = upload((void**)&d->rec, L.rec.data(), L.rec.size() * 4);
+	if (!rc) rc = upload((void**)&d->comps, L.comps.data(), L.comps.size() * 4);
+	if (!rc) rc = upload((void**)&d->lo_index, L.lo_index.data(), L.lo_index.size() * 4);
+	if (!rc && !(flags & SGI_BUILD_NO_FP64))
+	{
+		std::vector<double> s(nrow * d->ld, 0.0);
+		for (int n = 0; n < g.nno; n++)
+			memcpy(&s[(size_t)n * d->ld], &g.surplus[(size_t)n * g.TotalDof], sizeof(double) * g.TotalDof);
+		rc = upload((void**)&d->s64, s.data(), s.size() * 8);
+	}
+	if (!rc && (flags & (SGI_BUILD_FP32 | SGI_BUILD_NO_FP64)))
+	{
+		std::vector<float> hi(nrow * d->ld, 0.f), lo((size_t)std::max(L.ncoarse, 1) * d->ld, 0.f);
+		for (int n = 0; n < g.nno; n++)
+			for (int o = 0; o < g.TotalDof; o++)
+			{
+				const double v = g.surplus[(size_t)n * g.TotalDof + o];
+				const float h = (float)v;
+				hi[(size_t)n * d->ld + o] = h;
+				if (L.lo_index[n] != ~0u) lo[(size_t)L.lo_index[n] * d->ld + o] = (float)(v - (double)h);
+			}
+		rc = upload((void**)&d->s32, hi.data(), hi.size() * 4);
+		if (!rc) rc = upload((void**)&d->s32lo, lo.data(), lo.size() * 4);
+	}
+	if (rc) { free_grid(d); return rc; }
+	sgi_grid_info& I = d->info;
+	I.dim = g.dim; I.nno = g.nno; I.TotalDof = g.TotalDof; I.ld = d->ld;
+	I.max_comps = L.max_comps; I.tree_depth = L.tree_depth; I.tree_roots = L.tree_roots;
+	I.multi_delta = L.multi_delta; I.ncoarse = L.ncoarse; I.comps = (long long)L.comps.size() / 2;
+	I.device_bytes = bytes; I.coarse_threshold = L.coarse_threshold;
+	*out = d;
+	return SGI_OK;
+}
+
+extern "C" int sgi_grid_info_get(sgi_grid_t g, sgi_grid_info* info)
+{
+	clear_error();
+	if (!g || !info) return fail(SGI_E_INVALID, "null argument");
+	*info = g->info;
+	return SGI_OK;
+}
+
+extern "C" void sgi_grid_destroy(sgi_grid_t g) { free_grid(g); }
+
+extern "C" int sgi_last_launch(sgi_launch_stats* s)
+{
+	if (!s) return fail(SGI_E_INVALID, "null argument");
+	*s = g_stats;
+	return SGI_OK;
+}
+
+namespace {
+
+int check_set(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets)
+{
+	if (ngrids < 1 || !grids || !pt_offsets) return fail(SGI_E_INVALID, "empty grid set");
+	for (int k = 0; k < ngrids; k++)
+	{
+		if (!grids[k]) return fail(SGI_E_INVALID, "grid %d is null", k);
+		if (grids[k]->device != grids[0]->device) return fail(SGI_E_INVALID, "grids on different devices");
+		if (grids[k]->dim != grids[0]->dim)
+			return fail(SGI_E_MISMATCH, "state %d has dim %d, state 0 has %d", k, grids[k]->dim, grids[0]->dim);
+		if (grids[k]->TD != grids[0]->TD)
+			return fail(SGI_E_MISMATCH, "state %d TotalDof (%d) mismatches state 0 (%d)", k, grids[k]->TD, grids[0]->TD);
+		if (pt_offsets[k + 1] < pt_offsets[k]) return fail(SGI_E_INVALID, "point offsets decrease at %d", k);
+	}
+	if (pt_offsets[0] != 0) return fail(SGI_E_INVALID, "pt_offsets[0] must be 0");
+	return SGI_OK;
+}
+
+int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets, const double* x,
+	double* out, int precision, cudaStream_t stream)
+{
+	const sgi_grid* g0 = grids[0];
+	DeviceWork* W = nullptr;
+	int rc = device_work(g0->device, &W);
+	if (rc) return rc;
+	if (precision == SGI_FP64) { for (int k = 0; k < ngrids; k++) if (!grids[k]->s64) return fail(SGI_E_INVALID, "grid %d has no FP64 surplus", k); }
+	else if (precision == SGI_FP32C) { for (int k = 0; k < ngrids; k++) if (!grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k); }
+	else return fail(SGI_E_INVALID, "unknown precision %d", precision);
+	const size_t smem = (size_t)WARPS * g0->dim * sizeof(double);
+	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
+	g_stats = sgi_launch_stats{};
+	for (int gb = 0; gb < ngrids; gb += MAXG)
+	{
+		const int ng = std::min(MAXG, ngrids - gb);
+		const long long p0 = pt_offsets[gb], p1 = pt_offsets[gb + ng];
+		if (p1 == p0) continue;
+		FwdArgs a;
+		memset(&a, 0, sizeof(a));
+		for (int k = 0; k < ng; k++) a.g[k] = desc_of(grids[gb + k], pt_offsets[gb + k] - p0);
+		a.x = x + (size_t)p0 * g0->dim;
+		a.out = out + (size_t)p0 * g0->TD;
+		a.npts = p1 - p0;
+		a.ngrids = ng; a.dim = g0->dim; a.TD = g0->TD;
+		for (int ob = 0; ob < g0->TD; ob += 32 * RMAX)
+		{
+			a.o_begin = ob;
+			const int R = pick_R(std::min(g0->TD - ob, 32 * RMAX));
+			a.counter = W->counters + (W->next.fetch_add(1) % NCOUNTERS);
+			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
+			void (*kern)(FwdArgs) = nullptr;
+			if (precision == SGI_FP64)
+				kern = R == 1 ? fwd_f64_kernel<1> : R == 2 ? fwd_f64_kernel<2> : R == 4 ? fwd_f64_kernel<4> : fwd_f64_kernel<8>;
+			else
+				kern = R == 1 ? fwd_f32c_kernel<1> : R == 2 ? fwd_f32c_kernel<2> : R == 4 ? fwd_f32c_kernel<4> : fwd_f32c_kernel<8>;
+			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			int blocks = 0;
+			rc = occupancy_grid(kern, smem, W->sms, &blocks);
+			if (rc) return rc;
+			const long long need = (a.npts + WARPS - 1) / WARPS;
+			if (blocks > need) blocks = (int)need;
+			kern<<<blocks, BLOCK, smem, stream>>>(a);
+			CUDA_TRY(cudaGetLastError());
+			g_stats.kernels++;
+			g_stats.grid_blocks = blocks;
+			g_stats.block_threads = BLOCK;
+		}
+		g_stats.points += a.npts;
+	}
+	return SGI_OK;
+}
+
+} // namespace
+
+extern "C" int sgi_interpolate(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, int precision, void* stream)
+{
+	clear_error();
+	int rc = check_set(ngrids, grids, pt_offsets);
+	if (rc) return rc;
+	if (pt_offsets[ngrids] > 0 && (!x || !out)) return fail(SGI_E_INVALID, "null x or out");
+	DeviceGuard guard(grids[0]->device);
+	return launch_forward(ngrids, grids, pt_offsets, x, out, precision, (cudaStream_t)stream);
+}
+
+extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, int precision)
+{
+	clear_error();
+	int rc = check_set(ngrids, grids, pt_offsets);
+	if (rc) return rc;
+	const long long npts = pt_offsets[ngrids];
+	if (npts > 0 && (!x || !out)) return fail(SGI_E_INVALID, "null x or out");
+	if (npts == 0) return SGI_OK;
+	const sgi_grid* g0 = grids[0];
+	DeviceGuard guard(g0->device);
+	DeviceWork* W = nullptr;
+	rc = device_work(g0->device, &W);
+	if (rc) return rc;
+	std::lock_guard<std::mutex> lk(W->mtx);
+	if (!W->stream) CUDA_TRY(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
+	const size_t xb = (size_t)npts * g0->dim * sizeof(double), ob = (size_t)npts * g0->TD * sizeof(double);
+	if (W->dx_bytes < xb) { cudaFree(W->dx); W->dx = nullptr; W->dx_bytes = 0; CUDA_TRY(cudaMalloc(&W->dx, xb)); W->dx_bytes = xb; }
+	if (W->dout_bytes < ob) { cudaFree(W->dout); W->dout = nullptr; W->dout_bytes = 0; CUDA_TRY(cudaMalloc(&W->dout, ob)); W->dout_bytes = ob; }
+	CUDA_TRY(cudaMemcpyAsync(W->dx, x, xb, cudaMemcpyHostToDevice, W->stream));
+	rc = launch_forward(ngrids, grids, pt_offsets, W->dx, W->dout, precision, W->stream);
+	if (rc) return rc;
+	CUDA_TRY(cudaMemcpyAsync(out, W->dout, ob, cudaMemcpyDeviceToHost, W->stream));
+	CUDA_TRY(cudaStreamSynchronize(W->stream));
+	return SGI_OK;
+}
+
+extern "C" int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream)
+{
+	clear_error();
+	if (!g || npts < 0 || (npts && (!x || !out))) return fail(SGI_E_INVALID, "bad arguments");
+	if (!npts) return SGI_OK;
+	DeviceGuard guard(g->device);
+	DeviceWork* W = nullptr;
+	int rc = device_work(g->device, &W);
+	if (rc) return rc;
+	FwdArgs a;
+	memset(&a, 0, sizeof(a));
+	a.g[0] = desc_of(g, 0);
+	a.x = x; a.npts = npts; a.ngrids = 1; a.dim = g->dim; a.TD = g->TD;
+	a.counter = W->counters + (W->next.fetch_add(1) % NCOUNTERS);
+	cudaStream_t s = (cudaStream_t)stream;
+	CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s));
+	const size_t smem = (size_t)WARPS * g->dim * sizeof(double);
+	if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	int blocks = 0;
+	rc = occupancy_grid(count_kernel, smem, W->sms, &blocks);
+	if (rc) return rc;
+	count_kernel<<<blocks, BLOCK, smem, s>>>(a, out);
+	CUDA_TRY(cudaGetLastError());
+	return SGI_OK;
+}
+
+extern "C" int sgi_backward(sgi_grid_t g, long long npts, const double* x, const double* gout,
+	double* gx, double* gsurplus, void* stream_)
+{
+	clear_error();
+	if (!g || npts < 0 || (npts && (!x || !gout))) return fail(SGI_E_INVALID, "bad arguments");
+	if (!g->s64) return fail(SGI_E_INVALID, "grid has no FP64 surplus");
+	if (g->TD > 32 * RMAX) return fail(SGI_E_RANGE, "backward supports TotalDof <= %d", 32 * RMAX);
+	if (npts > 0xffffffffll) return fail(SGI_E_RANGE, "too many points");
+	cudaStream_t stream = (cudaStream_t)stream_;
+	DeviceGuard guard(g->device);
+	DeviceWork* W = nullptr;
+	int rc = device_work(g->device, &W);
+	if (rc) return rc;
+	g_stats = sgi_launch_stats{};
+	if (gsurplus && (npts == 0 || g->nno == 0))
+	{
+		CUDA_TRY(cudaMemsetAsync(gsurplus, 0, sizeof(double) * (size_t)g->nno * g->TD, stream));
+		gsurplus = nullptr;
+	}
+	if (npts == 0) return SGI_OK;
+	const int R = pick_R(g->TD);
+	void (*pk)(BwdArgs) = R == 1 ? bwd_points_kernel<1> : R == 2 ? bwd_points_kernel<2> : R == 4 ? bwd_points_kernel<4> : bwd_points_kernel<8>;
+	const size_t smem = (size_t)WARPS * 2 * g->dim * sizeof(double);
+	if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	int blocks = 0;
+	rc = occupancy_grid(pk, smem, W->sms, &blocks);
+	if (rc) return rc;
+
+	BwdArgs a;
+	memset(&a, 0, sizeof(a));
+	a.G = desc_of(g, 0);
+	a.x = x; a.gout = gout; a.gx = gx; a.npts = npts; a.dim = g->dim; a.TD = g->TD;
+
+	// scratch (stream-ordered allocations)
+	long long* counts = nullptr;
+	long long* offs = nullptr;
+	uint32_t *pn = nullptr, *pp = nullptr, *order = nullptr, *order_sorted = nullptr, *node_sorted = nullptr;
+	double* pw = nullptr;
+	void* tmp = nullptr;
+	long long npairs = 0;
+	auto cleanup = [&]()
+	{
+		cudaFreeAsync(counts, stream); cudaFreeAsync(offs, stream); cudaFreeAsync(pn, stream);
+		cudaFreeAsync(pp, stream); cudaFreeAsync(pw, stream); cudaFreeAsync(order, stream);
+		cudaFreeAsync(order_sorted, stream); cudaFreeAsync(node_sorted, stream); cudaFreeAsync(tmp, stream);
+	};
+#define BWD_TRY(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { cleanup(); \
+	return fail(SGI_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); } } while (0)
+	if (gsurplus)
+	{
+		BWD_TRY(cudaMallocAsync((void**)&counts, sizeof(long long) * (npts + 1), stream));
+		BWD_TRY(cudaMallocAsync((void**)&offs, sizeof(long long) * (npts + 1), stream));
+		BWD_TRY(cudaMemsetAsync(counts + npts, 0, sizeof(long long), stream));
+		rc = sgi_active_count(g, npts, x, counts, stream);
+		if (rc) { cleanup(); return rc; }
+		size_t tb = 0;
+		BWD_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, counts, offs, npts + 1, stream));
+		BWD_TRY(cudaMallocAsync(&tmp, tb, stream));
+		BWD_TRY(cub::DeviceScan::ExclusiveSum(tmp, tb, counts, offs, npts + 1, stream));
+		BWD_TRY(cudaMemcpyAsync(&npairs, offs + npts, sizeof(long long), cudaMemcpyDeviceToHost, stream));
+		BWD_TRY(cudaStreamSynchronize(stream));
+		cudaFreeAsync(tmp, stream); tmp = nullptr;
+		if (npairs > 0x7fffffffll) { cleanup(); return fail(SGI_E_RANGE, "%lld active pairs exceed 2^31", npairs); }
+		const size_t np = (size_t)std::max(npairs, 1ll);
+		BWD_TRY(cudaMallocAsync((void**)&pn, 4 * np, stream));
+		BWD_TRY(cudaMallocAsync((void**)&pp, 4 * np, stream));
+		BWD_TRY(cudaMallocAsync((void**)&pw, 8 * np, stream));
+		a.pair_off = offs; a.pair_node = pn; a.pair_point = pp; a.pair_w = pw;
+	}
+	a.counter = W->counters + (W->next.fetch_add(1) % NCOUNTERS);
+	BWD_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
+	pk<<<blocks, BLOCK, smem, stream>>>(a);
+	BWD_TRY(cudaGetLastError());
+	g_stats.kernels++;
+	if (gsurplus)
+	{
+		const size_t np = (size_t)std::max(npairs, 1ll);
+		BWD_TRY(cudaMallocAsync((void**)&order, 4 * np, stream));
+		BWD_TRY(cudaMallocAsync((void**)&order_sorted, 4 * np, stream));
+		BWD_TRY(cudaMallocAsync((void**)&node_sorted, 4 * np, stream));
+		iota_kernel<<<W->sms * 4, 256, 0, stream>>>(order, npairs);
+		size_t tb = 0;
+		int endbit = 1;
+		while (endbit < 32 && (1ll << endbit) <= (long long)g->nno) endbit++;
+		BWD_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, pn, node_sorted, order, order_sorted, (int)npairs, 0, endbit, stream));
+		BWD_TRY(cudaMallocAsync(&tmp, tb, stream));
+		BWD_TRY(cub::DeviceRadixSort::SortPairs(tmp, tb, pn, node_sorted, order, order_sorted, (int)npairs, 0, endbit, stream));
+		void (*sk)(const uint32_t*, const uint32_t*, const uint32_t*, const double*, long long, const double*, double*, int, int) =
+			R == 1 ? bwd_surplus_kernel<1> : R == 2 ? bwd_surplus_kernel<2> : R == 4 ? bwd_surplus_kernel<4> : bwd_surplus_kernel<8>;
+		sk<<<W->sms * 8, BLOCK, 0, stream>>>(node_sorted, order_sorted, pp, pw, npairs, gout, gsurplus, g->nno, g->TD);
+		BWD_TRY(cudaGetLastError());
+		g_stats.kernels += 3;
+	}
+	cleanup();
+	g_stats.points = npts;
+	return SGI_OK;
+#undef BWD_TRY
+}

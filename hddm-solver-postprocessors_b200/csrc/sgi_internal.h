@@ -1,0 +1,66 @@
+// Internal declarations shared by the host layer (sgi_host.cpp), the device
+// layer (sgi_device.cu) and the plugin surface (plugin.cpp).
+#ifndef SGI_INTERNAL_H
+#define SGI_INTERNAL_H
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "sgi.h"
+
+namespace sgi {
+
+// Thread-local error message; returns `code` so callers can `return fail(...)`.
+int fail(int code, const char* fmt, ...);
+void clear_error();
+
+// A grid in the reference's dense form (see sgi.h).
+struct HostGrid
+{
+	int dim = 0, nno = 0, TotalDof = 0, Level = 0;
+	std::vector<int> index;      // nno * 2 * dim
+	std::vector<double> surplus; // nno * TotalDof
+};
+
+// ---------------------------------------------------------------- device layout
+//
+// Node record, 16 bytes, one per node in grid order:
+//   x: skip      index of the first node after this node's subtree
+//   y: comp_ptr  first component of this node in `comps`
+//   z: ncomp (bits 0-7) | flags (bits 8-15) | dim of the delta component (16-31)
+//   w: i (bits 0-15) | j (bits 16-31) of the delta component
+// A component is (dim, i, j) packed as uint2 {dim, i | j << 16}; a node's
+// components are its non-constant dimensions in increasing dimension order.
+enum NodeFlags : uint32_t
+{
+	NODE_ALWAYS = 1u << 8,  // no components: weight 1 everywhere
+	NODE_DEAD   = 1u << 9,  // a component with i = 0, j != 0: weight 0 everywhere
+	NODE_MULTI  = 1u << 10, // activity needs all components checked
+	NODE_COARSE = 1u << 11, // FP32 form keeps a lo row for this node
+};
+
+struct DeviceLayout
+{
+	std::vector<uint32_t> rec;   // 4 * nno
+	std::vector<uint32_t> comps; // 2 * ncomps
+	std::vector<uint32_t> lo_index; // nno: row in the lo array, or ~0u
+	std::vector<int> parent;        // nno: tree parent, or -1
+	int max_comps = 0, tree_depth = 0, tree_roots = 0, multi_delta = 0, ncoarse = 0;
+	double coarse_threshold = 0.0;
+};
+
+// Builds the containment tree over the grid's node order and the records.
+int build_layout(const HostGrid& g, DeviceLayout& L);
+
+// Rows whose largest |surplus| is at least this keep an FP32 lo row.
+double coarse_threshold_for(const HostGrid& g);
+
+} // namespace sgi
+
+struct sgi_host_grid
+{
+	sgi::HostGrid g;
+};
+
+#endif

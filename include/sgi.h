@@ -1,0 +1,187 @@
+/*
+ * sgi.h — C ABI of the B200 sparse-grid linear-basis interpolator.
+ *
+ * The hot path of the HDDM LinearBasis postprocessor: for every query point x,
+ *
+ *     value[o] = sum over grid nodes n of surplus[n][o] * prod_d phi(x_d; i_nd, j_nd)
+ *     phi(x; i, j) = max(0, 1 - |x*i - j|)          (i = 0, j = 0: phi = 1)
+ *
+ * on one GPU.  Plain pointers and sizes only; every entry point returns 0
+ * (SGI_OK) or a negative SGI_E* code, with a message for the calling thread in
+ * sgi_last_error().  Device pointers are CUDA device (or managed) memory on the
+ * grid's device; `stream` is a cudaStream_t (NULL = legacy default stream).
+ *
+ * Which reference interface each entry point replaces is cited per function
+ * (paths relative to the reference project apc-llc/hddm-solver-postprocessors).
+ * The reference's own plugin exports (getInterpolator, getData, ...) are
+ * declared in sgi_plugin.h.
+ */
+#ifndef SGI_H
+#define SGI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define SGI_OK             0
+#define SGI_E_INVALID     -1   /* bad argument (null pointer, negative size, ...) */
+#define SGI_E_MISMATCH    -2   /* DofPerNode / dim mismatch between call and grid */
+#define SGI_E_FORMAT      -3   /* malformed or unreadable grid file */
+#define SGI_E_RANGE       -4   /* value outside what the device layout encodes */
+#define SGI_E_CUDA        -5   /* CUDA runtime error */
+#define SGI_E_NOMEM       -6   /* host or device allocation failed */
+#define SGI_E_NODEVICE    -7   /* no CUDA device */
+#define SGI_E_DEVICE      -8   /* a kernel reported an error through its status word */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* sgi_last_error(void);
+
+/* Number of CUDA devices (0 when none).  Replaces the GPU count of
+ * LinearBasis/cuda/src/Devices.cu:13-47 / supported.cpp:13-20. */
+int sgi_device_count(void);
+
+/* ---------------------------------------------------------- host grids */
+/* A grid in the reference's dense form (LinearBasis/gold/include/Data.h:252):
+ * for node n and dimension k, index[n*2*dim + k] = i (0 for level 1) and
+ * index[n*2*dim + dim + k] = j; surplus[n*TotalDof + o].  Owned by the
+ * library. */
+typedef struct sgi_host_grid* sgi_host_grid_t;
+
+/* Read a .plt grid file in any of the reference's layouts (compressed,
+ * binary, text); `nagents` is the configured dimension, which the file's
+ * header must match.  Replaces DataDense::load's reader,
+ * LinearBasis/gold/src/Data.cpp:322-595. */
+int sgi_host_grid_read_plt(const char* path, int nagents, sgi_host_grid_t* out);
+
+/* Write the compressed .plt layout (marker "compressed", header, CSR index
+ * block of {u16 i, u16 j} pairs, CSR surplus block) that
+ * LinearBasis/gold/src/Data.cpp:49-190 reads.  No reference counterpart
+ * (the reference only reads). */
+int sgi_host_grid_write_plt(sgi_host_grid_t g, const char* path);
+
+/* Wrap caller arrays (copied). */
+int sgi_host_grid_from_dense(int dim, int nno, int TotalDof, const int* index,
+	const double* surplus, sgi_host_grid_t* out);
+
+/* Views of the arrays (valid until sgi_host_grid_free). */
+int sgi_host_grid_view(sgi_host_grid_t g, int* dim, int* nno, int* TotalDof,
+	const int** index, const double** surplus);
+void sgi_host_grid_free(sgi_host_grid_t g);
+
+/* Synthetic grids (no reference counterpart; the reference's large test grids
+ * are not in its tree).  Nodes are emitted in depth-first order of their
+ * refinement tree.  Surpluses are uniform[-1,1] * 2^(-2*sum_k(l_k-1)).
+ *   regular:  all nodes with sum_k (l_k - 1) <= level - 1
+ *   adaptive: from the level-1 root, repeatedly pick a uniformly random leaf
+ *             and add all its children along a random non-empty subset of
+ *             dimensions (each kept with probability p_dim), skipping children
+ *             above max_level, until nno nodes exist. */
+int sgi_gen_regular(int dim, int level, int TotalDof, uint64_t seed, sgi_host_grid_t* out);
+int sgi_gen_adaptive(int dim, int nno, int TotalDof, int max_level, double p_dim,
+	uint64_t seed, sgi_host_grid_t* out);
+
+/* Query points: kind 0 = uniform [0,1]^dim, 1 = N(0.5, 0.05^2) clipped to
+ * [0,1], 2 = first half uniform and second half clustered.  If kink_reject > 0,
+ * points with any coordinate within kink_reject of a multiple of
+ * 2^-(max_level-1) (a superset of every hat's kinks) are redrawn.  out is
+ * npts x dim, row-major. */
+int sgi_gen_points(int dim, long npts, int kind, uint64_t seed, double kink_reject,
+	int max_level, double* out);
+
+/* The reference x86 loader's sparse form of one grid (xps = unique
+ * (i, j, dim) triples with id 0 = empty; chains = per-node xps ids,
+ * 0-terminated, nfreqs per node; rows reordered).  Reproduces
+ * DataSparse::load, LinearBasis/x86/src/Data.cpp:598-951, bit for bit.
+ * Call with null arrays first to get nfreqs and szxps.
+ *   xps[3*k + {0,1,2}] = i, j, dim      (szxps triples)
+ *   chains[n*nfreqs + f]                (nno * nfreqs)
+ *   row_perm[r] = input row stored at reordered row r  (nno) */
+int sgi_host_grid_xps_chains(sgi_host_grid_t g, int* nfreqs, int* szxps,
+	int* xps, int* chains, int* row_perm);
+
+/* The containment tree the kernels walk (for inspection and tests): for node
+ * n in grid order, parent[n] is the nearest earlier node whose support holds
+ * n's support and that is still open on the depth-first stack (-1 if none),
+ * and n's subtree is the index range [n, skip[n]).  No reference counterpart. */
+int sgi_host_grid_tree(sgi_host_grid_t g, int* skip, int* parent);
+
+/* --------------------------------------------------------- device grids */
+typedef struct sgi_grid* sgi_grid_t;
+
+/* Build flags */
+#define SGI_BUILD_FP32    0x1u   /* also keep the FP32 hi (+ lo for coarse rows) surplus */
+#define SGI_BUILD_NO_FP64 0x2u   /* drop the FP64 surplus (FP32 forms only)              */
+
+typedef struct sgi_grid_info
+{
+	int dim, nno, TotalDof;
+	int ld;               /* surplus row stride on the device (elements)          */
+	int max_comps;        /* most non-constant dimensions of any node (nfreqs)    */
+	int tree_depth;       /* depth of the containment tree                       */
+	int tree_roots;       /* nodes without a containing ancestor                  */
+	int multi_delta;      /* nodes that differ from their tree parent in >1 dim   */
+	int ncoarse;          /* rows kept as FP32 hi+lo                              */
+	long long comps;      /* stored (dim, i, j) components                        */
+	long long device_bytes;
+	double coarse_threshold;
+} sgi_grid_info;
+
+/* Upload a grid to `device`.  Nodes keep the host grid's order, so the FP64
+ * forward form adds node contributions in file order, as the reference's gold
+ * kernel does.  Replaces the device upload of cuda Data::load,
+ * LinearBasis/cuda/src/Data.cu:348-949. */
+int sgi_grid_create(sgi_host_grid_t g, int device, unsigned flags, sgi_grid_t* out);
+int sgi_grid_info_get(sgi_grid_t g, sgi_grid_info* info);
+void sgi_grid_destroy(sgi_grid_t g);
+
+/* ---------------------------------------------------------- interpolate */
+#define SGI_FP64   0   /* plain FP64: node order and rounding of the gold kernel */
+#define SGI_FP32C  1   /* FP32 surplus products, hi/lo coarse rows, compensated sums, FP64 final */
+
+/* Batched forward over a set of grids sharing dim and TotalDof (a multistate
+ * set or a single grid): grid g owns points [pt_offsets[g], pt_offsets[g+1]).
+ * x: device, pt_offsets[ngrids] x dim; out: device, pt_offsets[ngrids] x
+ * TotalDof.  pt_offsets is HOST memory.  One persistent launch pulls points
+ * from a device work queue.  Replaces LinearBasis_cuda_Generic_InterpolateArray
+ * (LinearBasis/cuda/src/InterpolateArray.cu:239-267, one point per call) and
+ * ..._InterpolateArrayManyMultistate (InterpolateArrayManyMultistate.cu:346-395,
+ * one point per state per call). */
+int sgi_interpolate(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, int precision, void* stream);
+
+/* Same with HOST x/out: stages through pinned buffers, copies in, launches,
+ * copies out and synchronizes — the reference plugin's per-call contract
+ * (include/interpolator.h:32-37, host x and value arrays). */
+int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, int precision);
+
+/* Backward of the FP64 form for one grid: given gout = dL/dvalue (npts x
+ * TotalDof, device), writes gx = dL/dx (npts x dim, device; may be NULL) and
+ * gsurplus = dL/dsurplus (nno x TotalDof in file row order, device; may be
+ * NULL; overwritten).  Weights are recomputed, never stored; dL/dsurplus is
+ * reduced without atomics.  No reference counterpart. */
+int sgi_backward(sgi_grid_t g, long long npts, const double* x, const double* gout,
+	double* gx, double* gsurplus, void* stream);
+
+/* Active-node count A(x) per point (device int64 out[npts]); diagnostics. */
+int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream);
+
+/* Launch statistics of this thread's last sgi_interpolate/sgi_backward call. */
+typedef struct sgi_launch_stats
+{
+	int kernels;          /* kernels launched by the call                 */
+	int grid_blocks;
+	int block_threads;
+	long long points;
+} sgi_launch_stats;
+int sgi_last_launch(sgi_launch_stats* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SGI_H */

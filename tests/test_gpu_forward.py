@@ -1,0 +1,185 @@
+"""Forward kernels on the GPU against the oracle (gold restatement, pinned to
+the reference's known answers and to the reference's own gold kernel).
+
+FP64 form: bit-identical to gold (same node order, same multiplies and adds).
+FP32C form: max relative error <= 1e-7 against gold, with the error metric
+max_o |a - b| / max(|b_o|, 1e-3 * max_o |b_o|) per point.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import hddm_b200 as H
+import oracle as O
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+PLT = os.path.join(GOLDEN, "interpolate_array_surplus.plt")
+DOC = json.load(open(os.path.join(GOLDEN, "interpolate_array.json")))
+FP32C_TOL = 1e-7
+
+
+def _run(grid, X, precision=H.FP64, counts=None):
+    import torch
+    x = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    out = H.interpolate(grid, x, counts=counts, precision=precision)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def test_reference_known_answer_fixture_bit_exact(cuda):
+    hg = H.HostGrid.read_plt(PLT, 59)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    x = np.array(DOC["x"])[None, :]
+    v = _run(g, x)[0]
+    assert np.array_equal(v, np.array(DOC["ref_gold"]))
+    assert np.abs(v - np.array(DOC["expected_test_cpp"])).max() < DOC["epsilon_test_cpp"]
+    v32 = _run(g, x, H.FP32C)
+    assert O.rel_error(v32, np.array(DOC["ref_gold"])[None])[0] <= FP32C_TOL
+    # the host-pointer entry point gives the same bits
+    assert np.array_equal(H.interpolate_host(g, x)[0], v)
+
+
+def test_config0_regular_d4_bit_exact(cuda):
+    hg = H.HostGrid.regular(4, 4, 8, seed=0)
+    assert hg.nno == 137
+    X = H.gen_points(4, 1024, kind=0, seed=0)
+    ref = O.Gold(*hg.arrays()).interpolate(X)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    assert np.array_equal(_run(g, X), ref)
+    assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
+
+
+def test_config1_regular_d16_bit_exact(cuda):
+    hg = H.HostGrid.regular(16, 5, 32, seed=1)
+    assert hg.nno == 51137
+    X = H.gen_points(16, 65536, kind=0, seed=1)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    out = _run(g, X)
+    sub = np.random.default_rng(11).choice(len(X), 2048, replace=False)
+    ref = O.Gold(*hg.arrays()).interpolate(X[sub])
+    assert np.array_equal(out[sub], ref)
+    e32 = O.rel_error(_run(g, X, H.FP32C), out)
+    assert e32[0] <= FP32C_TOL, e32
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_adaptive_d59_bit_exact(cuda, kind):
+    hg = H.HostGrid.adaptive(59, 30000, 64, seed=3)
+    X = H.gen_points(59, 512, kind=kind, seed=kind + 20)
+    ref = O.Gold(*hg.arrays()).interpolate(X)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    assert np.array_equal(_run(g, X), ref)
+    assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
+
+
+def test_td256_multi_pass_and_ragged_td(cuda):
+    for td in (118, 256, 300, 5):
+        hg = H.HostGrid.adaptive(12, 3000, td, seed=td)
+        X = H.gen_points(12, 300, kind=2, seed=td)
+        ref = O.Gold(*hg.arrays()).interpolate(X)
+        g = H.Grid(hg, flags=H.BUILD_FP32)
+        assert np.array_equal(_run(g, X), ref), td
+        assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL, td
+
+
+def test_multistate_ragged_batch_one_launch(cuda):
+    """8 grids of uneven size, ragged point counts (including 0 and 1), one call."""
+    rng = np.random.default_rng(2)
+    hosts = [H.HostGrid.adaptive(30, int(n), 64, seed=100 + k)
+             for k, n in enumerate(np.exp(rng.uniform(np.log(2000), np.log(20000), 8)).astype(int))]
+    grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
+    counts = [37, 0, 1, 500, 3, 1200, 64, 9]
+    X = H.gen_points(30, sum(counts), kind=0, seed=7)
+    out = _run(grids, X, counts=counts)
+    out32 = _run(grids, X, H.FP32C, counts=counts)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for k, h in enumerate(hosts):
+        seg = slice(off[k], off[k + 1])
+        if counts[k] == 0:
+            continue
+        ref = O.Gold(*h.arrays()).interpolate(X[seg])
+        assert np.array_equal(out[seg], ref), k
+        assert O.rel_error(out32[seg], ref)[0] <= FP32C_TOL, k
+        assert np.array_equal(_run(grids[k], X[seg]), ref)
+    # the reference's multistate call shape: one point per state
+    X1 = H.gen_points(30, 8, kind=0, seed=8)
+    out1 = _run(grids, X1, counts=[1] * 8)
+    for k, h in enumerate(hosts):
+        assert np.array_equal(out1[k], O.Gold(*h.arrays()).interpolate(X1[k])[0])
+
+
+def test_edge_cases(cuda):
+    import torch
+    # root-only grid, a never-active node, duplicated node, points outside [0, 1]
+    dim = 3
+    index = np.array([[0, 0, 0, 0, 0, 0],
+                      [2, 0, 0, 0, 0, 0],
+                      [0, 0, 0, 5, 0, 0],     # i = 0, j = 5: weight 1 - 5 < 0 everywhere
+                      [2, 0, 0, 0, 0, 0],     # duplicate of node 1
+                      [4, 2, 0, 1, 0, 0],
+                      [4, 2, 0, 1, 2, 0]], np.int32)
+    sur = np.arange(6 * 3, dtype=np.float64).reshape(6, 3) / 7.0 - 1.0
+    hg = H.HostGrid.from_dense(index, sur)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    X = np.array([[0.1, 0.2, 0.3], [0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [0.5, 0.5, 0.5],
+                  [0.25, 0.25, 0.25], [-0.3, 1.7, 0.5], [0.125, 0.5 - 1e-17, 0.99]])
+    ref = O.Gold(index, sur).interpolate(X)
+    assert np.array_equal(_run(g, X), ref)
+    assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
+    # root-only grid
+    g1 = H.Grid(H.HostGrid.from_dense(index[:1], sur[:1]))
+    assert np.array_equal(_run(g1, X), np.repeat(sur[:1], len(X), axis=0))
+    # non-finite coordinates: gold multiplies NaN into every node
+    Xn = np.array([[np.nan, 0.1, 0.2], [0.1, np.inf, 0.2]])
+    assert np.isnan(_run(g, Xn)).all() and np.isnan(O.Gold(index, sur).interpolate(Xn)).all()
+    # empty batch
+    out = H.interpolate(g, torch.zeros((0, dim), dtype=torch.float64, device="cuda"))
+    assert out.shape == (0, 3)
+
+
+def test_grid_points_and_kinks_exact(cuda):
+    """Points on grid nodes and hat kinks (hats exactly 0 there)."""
+    hg = H.HostGrid.regular(5, 5, 16, seed=9)
+    r = np.random.default_rng(4)
+    X = r.integers(0, 17, size=(400, 5)) / 16.0
+    ref = O.Gold(*hg.arrays()).interpolate(X)
+    g = H.Grid(hg)
+    assert np.array_equal(_run(g, X), ref)
+
+
+def test_file_order_not_depth_first_still_exact(cuda):
+    """Rows in random order: the tree degrades (many roots), results stay exact."""
+    idx, sur = H.HostGrid.adaptive(16, 4000, 32, seed=5).arrays()
+    perm = np.random.default_rng(1).permutation(len(idx))
+    hg = H.HostGrid.from_dense(idx[perm], sur[perm])
+    g = H.Grid(hg)
+    assert g.info.tree_roots > 1
+    X = H.gen_points(16, 256, kind=0, seed=3)
+    assert np.array_equal(_run(g, X), O.Gold(idx[perm], sur[perm]).interpolate(X))
+
+
+def test_active_count_matches_oracle(cuda):
+    import torch
+    hg = H.HostGrid.adaptive(59, 20000, 4, seed=3)
+    X = H.gen_points(59, 64, kind=2, seed=6)
+    g = H.Grid(hg)
+    cnt = H.active_count(g, torch.from_numpy(X).cuda()).cpu().numpy()
+    og = O.Gold(*hg.arrays())
+    assert np.array_equal(cnt, [og.active_count(x) for x in X])
+
+
+def test_errors(cuda):
+    import torch
+    a = H.Grid(H.HostGrid.regular(4, 3, 8, 0))
+    b = H.Grid(H.HostGrid.regular(4, 3, 9, 0))
+    x = torch.zeros((2, 4), dtype=torch.float64, device="cuda")
+    with pytest.raises(H.SgiError) as e:
+        H.interpolate([a, b], x, counts=[1, 1])
+    assert e.value.code == -2 and "TotalDof" in str(e.value)
+    with pytest.raises(H.SgiError) as e:
+        H.interpolate(a, x, precision=H.FP32C)   # built without BUILD_FP32
+    assert e.value.code == -1
