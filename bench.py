@@ -127,14 +127,15 @@ def run_gpu(args):
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    hg, X, t_gen = make_workload(seed_offset=rank)
+    npts = args.points
+    hg, X, t_gen = make_workload(npts=npts, seed_offset=rank)
     t0 = time.time()
     grid = H.Grid(hg, device=local, flags=H.BUILD_FP32)
     t_upload = time.time() - t0
     info = grid.info
     x = torch.from_numpy(X).to(dev)
-    out32 = torch.empty((NPTS, TD), dtype=torch.float64, device=dev)
-    out64 = torch.empty((NPTS, TD), dtype=torch.float64, device=dev)
+    out32 = torch.empty((npts, TD), dtype=torch.float64, device=dev)
+    out64 = torch.empty((npts, TD), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
@@ -164,6 +165,9 @@ def run_gpu(args):
     den = torch.maximum(out64.abs(), 1e-3 * out64.abs().amax(dim=1, keepdim=True))
     perr = ((out32 - out64).abs() / den).amax(dim=1)
     err_max, err_rms = float(perr.max()), float(perr.pow(2).mean().sqrt())
+    if args.only_accuracy_pass:
+        print(json.dumps({"fp32c_max_rel_err": err_max, "fp32c_rms_rel_err": err_rms, "points": npts}))
+        return
     counts = H.active_count(grid, x[:65536], stream=stream).double()
     mean_active = float(counts.mean())
 
@@ -174,9 +178,9 @@ def run_gpu(args):
 
     # end to end through the C ABI's host-pointer entry: pinned x in, pinned out back
     xh = torch.from_numpy(X).pin_memory()
-    outh = torch.empty((NPTS, TD), dtype=torch.float64).pin_memory()
+    outh = torch.empty((npts, TD), dtype=torch.float64).pin_memory()
     import ctypes
-    offs = np.array([0, NPTS], np.int64)
+    offs = np.array([0, npts], np.int64)
     garr = (ctypes.c_void_p * 1)(grid.handle.value)
 
     def e2e_once():
@@ -205,13 +209,13 @@ def run_gpu(args):
     result = None
     if rank == 0:
         hbm, peak_kind = peaks()
-        b32, szxps = alg_bytes(hg, info, NPTS, 4)
-        b64, _ = alg_bytes(hg, info, NPTS, 8)
+        b32, szxps = alg_bytes(hg, info, npts, 4)
+        b64, _ = alg_bytes(hg, info, npts, 8)
         ms32 = t32 / args.steps
         ms64 = t64 / args.steps
         ach = b32 / (ms32 * 1e-3) / 1e9
-        pts_s = NPTS * world / (ms32 * 1e-3)
-        pts64_s = NPTS * world / (ms64 * 1e-3)
+        pts_s = npts * world / (ms32 * 1e-3)
+        pts64_s = npts * world / (ms64 * 1e-3)
         traffic = None
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
@@ -229,7 +233,7 @@ def run_gpu(args):
             "vs_baseline": None,
             "dtype": "f32+comp (f64 in/out)",
             "data": "synthetic: seeded adaptive grid and points (reference's large grids are not in its tree)",
-            "config": {"workload": WORKLOAD, "dim": DIM, "nno": info.nno, "TotalDof": TD, "points_per_gpu": NPTS,
+            "config": {"workload": WORKLOAD, "dim": DIM, "nno": info.nno, "TotalDof": TD, "points_per_gpu": npts,
                        "max_comps": info.max_comps, "ncoarse": info.ncoarse, "szxps": szxps,
                        "mean_active_nodes_per_point": mean_active,
                        "l2": "inputs larger than L2 (x 472 MB, surplus 1 GB FP32 / 2 GB FP64)",
@@ -238,15 +242,15 @@ def run_gpu(args):
             "fp64_form": {"points_per_s": pts64_s, "ms_per_step": ms64,
                           "roofline_frac": b64 / (ms64 * 1e-3) / 1e9 / hbm},
             "speedup_fp32c_vs_fp64_form": pts_s / pts64_s,
-            "fp32c_vs_gold_exact_fp64": {"max_rel_err": err_max, "rms_rel_err": err_rms, "points": NPTS},
+            "fp32c_vs_gold_exact_fp64": {"max_rel_err": err_max, "rms_rel_err": err_rms, "points": npts},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                          "peak_kind": f"{peak_kind} (burst copy)", "algorithmic_bytes_per_launch": b32,
                          "traffic": traffic, "kernel": "fwd_f32c_kernel"},
             "fma_work": {"mean_active_nodes": mean_active,
-                         "flops_per_launch": 2.0 * mean_active * TD * NPTS,
-                         "achieved_tflops": 2.0 * mean_active * TD * NPTS / (ms32 * 1e-3) / 1e12},
-            "e2e": {"value": NPTS * world / (t_e2e / args.steps * 1e-3), "unit": "points/s",
-                    "h2d_bytes_per_step": NPTS * DIM * 8, "d2h_bytes_per_step": NPTS * TD * 8},
+                         "flops_per_launch": 2.0 * mean_active * TD * npts,
+                         "achieved_tflops": 2.0 * mean_active * TD * npts / (ms32 * 1e-3) / 1e12},
+            "e2e": {"value": npts * world / (t_e2e / args.steps * 1e-3), "unit": "points/s",
+                    "h2d_bytes_per_step": npts * DIM * 8, "d2h_bytes_per_step": npts * TD * 8},
             "gpu_launches": args.steps * (k32 + k64),
             "clocks": clocks,
             "setup_s": {"generate": round(t_gen, 2), "layout_and_upload": round(t_upload, 2)},
@@ -274,7 +278,8 @@ def cpu_baseline(hg, X, sample, variant):
         r = O.RefGrid(p, DIM, variant)
         t_load = time.time() - t
         cores = os.cpu_count() or 1
-        sub = np.ascontiguousarray(X[:sample // 2].tolist() + X[NPTS // 2:NPTS // 2 + sample - sample // 2].tolist())
+        half = len(X) // 2
+        sub = np.ascontiguousarray(np.concatenate([X[:sample // 2], X[half:half + sample - sample // 2]]))
         r.interpolate(sub[:cores], nthreads=cores)
         t = time.perf_counter()
         r.interpolate(sub, nthreads=cores)
@@ -332,6 +337,9 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--points", type=int, default=NPTS, help="points per GPU (default: the workload's 1M)")
+    ap.add_argument("--only-accuracy-pass", action="store_true",
+                    help="run one FP64 and one FP32C launch, print their agreement and exit (profiling case)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

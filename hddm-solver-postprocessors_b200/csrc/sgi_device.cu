@@ -176,17 +176,33 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 		{
 			traverse(G, xs, lane, [&](unsigned mask, int n0, double w, const uint4&)
 			{
+				// two hits per step, both rows loaded before either is added, so
+				// that each warp keeps two rows in flight; the adds stay in order
 				while (mask)
 				{
-					const int k = __ffs(mask) - 1;
+					const int k0 = __ffs(mask) - 1;
 					mask &= mask - 1;
-					const double wk = __shfl_sync(FULL, w, k);
-					const double* row = G.s64 + (size_t)(n0 + k) * G.ld + a.o_begin;
+					const bool two = mask != 0u;
+					const int k1 = two ? __ffs(mask) - 1 : k0;
+					if (two) mask &= mask - 1;
+					const double w0 = __shfl_sync(FULL, w, k0);
+					const double w1 = __shfl_sync(FULL, w, k1);
+					const double* row0 = G.s64 + (size_t)(n0 + k0) * G.ld + a.o_begin;
+					const double* row1 = G.s64 + (size_t)(n0 + k1) * G.ld + a.o_begin;
+					double v0[R], v1[R];
 #pragma unroll
 					for (int r = 0; r < R; r++)
 					{
 						const int o = lane + 32 * r;
-						if (a.o_begin + o < G.ld) acc[r] = __dadd_rn(acc[r], __dmul_rn(wk, __ldg(row + o)));
+						const bool in = a.o_begin + o < G.ld;
+						v0[r] = in ? __ldg(row0 + o) : 0.0;
+						v1[r] = in && two ? __ldg(row1 + o) : 0.0;
+					}
+#pragma unroll
+					for (int r = 0; r < R; r++)
+					{
+						acc[r] = __dadd_rn(acc[r], __dmul_rn(w0, v0[r]));
+						if (two) acc[r] = __dadd_rn(acc[r], __dmul_rn(w1, v1[r]));
 					}
 				}
 			});
@@ -204,9 +220,9 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 
 // FP32 + compensated form.  Per output: a double-float accumulator (hi, lo)
 // for coarse rows, whose terms are formed from the hi/lo splits of weight and
-// surplus with an exact FMA product error, added with TwoSum; a plain FP32
-// FMA accumulator for the other rows; the three parts are summed in FP64 at
-// the end.
+// surplus with an exact FMA product error, added with TwoSum; a Kahan-
+// compensated FP32 accumulator for the other rows; the parts are summed in
+// FP64 at the end.
 template <int R>
 __global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__ FwdArgs a)
 {
@@ -220,9 +236,9 @@ __global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__
 		p = __shfl_sync(FULL, p, 0);
 		if (p >= a.npts) break;
 		const GridDesc& G = a.g[find_grid(a, p)];
-		float ch[R], cl[R], fa[R];
+		float ch[R], cl[R], fa[R], fc[R];
 #pragma unroll
-		for (int r = 0; r < R; r++) { ch[r] = 0.f; cl[r] = 0.f; fa[r] = 0.f; }
+		for (int r = 0; r < R; r++) { ch[r] = 0.f; cl[r] = 0.f; fa[r] = 0.f; fc[r] = 0.f; }
 		const bool ok = load_point(a, p, xs, lane);
 		if (ok)
 		{
@@ -244,31 +260,45 @@ __global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__
 					{
 						const float wlo = __double2float_rn(wk - (double)whi);
 						const float* rlo = G.s32lo + (size_t)lok * G.ld + a.o_begin;
+						float shi[R], slo[R];
 #pragma unroll
 						for (int r = 0; r < R; r++)
 						{
 							const int o = lane + 32 * r;
-							if (a.o_begin + o < G.ld)
-							{
-								const float shi = __ldg(row + o), slo = __ldg(rlo + o);
-								const float pr = __fmul_rn(whi, shi);
-								const float pe = __fmaf_rn(whi, shi, -pr);
-								const float tl = __fmaf_rn(whi, slo, __fmaf_rn(wlo, shi, pe));
-								const float s = __fadd_rn(ch[r], pr);
-								const float bp = __fsub_rn(s, ch[r]);
-								const float e = __fadd_rn(__fsub_rn(ch[r], __fsub_rn(s, bp)), __fsub_rn(pr, bp));
-								ch[r] = s;
-								cl[r] = __fadd_rn(cl[r], __fadd_rn(e, tl));
-							}
+							const bool in = a.o_begin + o < G.ld;
+							shi[r] = in ? __ldg(row + o) : 0.f;
+							slo[r] = in ? __ldg(rlo + o) : 0.f;
+						}
+#pragma unroll
+						for (int r = 0; r < R; r++)
+						{
+							const float pr = __fmul_rn(whi, shi[r]);
+							const float pe = __fmaf_rn(whi, shi[r], -pr);
+							const float tl = __fmaf_rn(whi, slo[r], __fmaf_rn(wlo, shi[r], pe));
+							const float s = __fadd_rn(ch[r], pr);
+							const float bp = __fsub_rn(s, ch[r]);
+							const float e = __fadd_rn(__fsub_rn(ch[r], __fsub_rn(s, bp)), __fsub_rn(pr, bp));
+							ch[r] = s;
+							cl[r] = __fadd_rn(cl[r], __fadd_rn(e, tl));
 						}
 					}
 					else
 					{
+						float sv[R];
 #pragma unroll
 						for (int r = 0; r < R; r++)
 						{
 							const int o = lane + 32 * r;
-							if (a.o_begin + o < G.ld) fa[r] = __fmaf_rn(whi, __ldg(row + o), fa[r]);
+							sv[r] = a.o_begin + o < G.ld ? __ldg(row + o) : 0.f;
+						}
+#pragma unroll
+						for (int r = 0; r < R; r++)
+						{
+							const float t = __fmul_rn(whi, sv[r]);
+							const float y = __fsub_rn(t, fc[r]);
+							const float s = __fadd_rn(fa[r], y);
+							fc[r] = __fsub_rn(__fsub_rn(s, fa[r]), y);
+							fa[r] = s;
 						}
 					}
 				}
@@ -280,7 +310,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__
 		{
 			const int o = lane + 32 * r;
 			if (a.o_begin + o < a.TD)
-				dst[o] = ok ? ((double)ch[r] + (double)cl[r]) + (double)fa[r]
+				dst[o] = ok ? (((double)ch[r] + (double)cl[r]) + ((double)fa[r] - (double)fc[r]))
 				            : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0);
 		}
 		__syncwarp();
