@@ -78,14 +78,11 @@ public :
 	int sms = 0;
 };
 
-class DeviceProperties
+size_t SIMDVector::getLength(size_t szelement) const
 {
-public :
-	const Device* device;
-	explicit DeviceProperties(const Device* d) : device(d) { }
-	virtual const void* getSIMDVector() const { return nullptr; }
-	virtual ~DeviceProperties() { }
-};
+	if (szelement == 4 || szelement == 8) return (size_t)device->warpSize;
+	die("Unsupported vector element size = %zu\n", szelement);
+}
 
 // Reads hddm-solver.cfg: "name value !comment" lines, the keys the CUDA
 // variant reads (LinearBasis/cuda/src/parameters.cpp:96-150).
@@ -124,17 +121,17 @@ Parameters::Parameters(const std::string& targetSuffix, const std::string& confi
 }
 
 // All states of one multistate set; each state a device grid.
-class Data
+class DataImpl : public Data
 {
 public :
 	int nstates, dim = 0, TotalDof = 0;
 	std::vector<sgi_grid_t> grids;
 	std::vector<bool> loaded;
 
-	explicit Data(int n) : nstates(n), grids(n, nullptr), loaded(n, false) { }
+	explicit DataImpl(int n) : nstates(n), grids(n, nullptr), loaded(n, false) { }
 
 	// LinearBasis/cuda/src/Data.cu:348-949 (via gold/src/Data.cpp:322-436 checks)
-	virtual void load(const char* filename, int istate)
+	void load(const char* filename, int istate) override
 	{
 		const Parameters& params = Interpolator::getInstance()->getParameters();
 		if (istate < 0 || istate >= nstates) die("State %d index out of range 0 .. %d\n", istate, nstates - 1);
@@ -162,7 +159,7 @@ public :
 		loaded[istate] = true;
 	}
 
-	virtual void clear()
+	void clear() override
 	{
 		for (int s = 0; s < nstates; s++)
 		{
@@ -172,7 +169,7 @@ public :
 		}
 	}
 
-	virtual ~Data() { clear(); }
+	~DataImpl() override { clear(); }
 };
 
 namespace {
@@ -194,16 +191,17 @@ Interpolator* Interpolator::getInstance()
 	return interp.get();
 }
 
-static void check_dof(const Data* data, int DofPerNode)
+static void check_dof(const DataImpl* data, int DofPerNode)
 {
 	if (DofPerNode != data->TotalDof)
 		die("Requested DofPerNode (%d) mismatches actual data TotalDof (%d)\n", DofPerNode, data->TotalDof);
 }
 
-void Interpolator::interpolate(Device* device, Data* data, const int istate, const real* x,
+void Interpolator::interpolate(Device* device, Data* data_, const int istate, const real* x,
 	const int DofPerNode, real* value)
 {
 	(void)device;
+	DataImpl* data = static_cast<DataImpl*>(data_);
 	check_dof(data, DofPerNode);
 	if (istate < 0 || istate >= data->nstates || !data->loaded[istate])
 		die("State %d is not loaded\n", istate);
@@ -212,9 +210,10 @@ void Interpolator::interpolate(Device* device, Data* data, const int istate, con
 	if (rc) die("%s\n", sgi_last_error());
 }
 
-void Interpolator::interpolate(Device* device, Data* data, const real** x, const int DofPerNode, real** value)
+void Interpolator::interpolate(Device* device, Data* data_, const real** x, const int DofPerNode, real** value)
 {
 	(void)device;
+	DataImpl* data = static_cast<DataImpl*>(data_);
 	check_dof(data, DofPerNode);
 	const int n = data->nstates;
 	for (int s = 0; s < n; s++) if (!data->loaded[s]) die("State %d is not loaded\n", s);
@@ -272,7 +271,7 @@ Devices& devices()
 
 extern "C" Interpolator* getInterpolator() { return Interpolator::getInstance(); }
 
-extern "C" Data* getData(int nstates) { return new Data(nstates); }
+extern "C" Data* getData(int nstates) { return new DataImpl(nstates); }
 
 extern "C" bool isSupported() { return sgi_device_count() > 0; }
 

@@ -27,7 +27,6 @@ namespace SGI_PLUGIN_NAMESPACE {
 typedef double real;
 
 class Device;
-class DeviceProperties;
 
 enum BasisType
 {
@@ -45,7 +44,49 @@ struct Parameters
 	Parameters(const std::string& targetSuffix, const std::string& configFile = "hddm-solver.cfg");
 };
 
-class Data;
+// A multistate set of grids (LinearBasis/cuda/include/Data.h:482-551: virtual
+// load, virtual clear, virtual destructor, in that vtable order).  getData()
+// returns the library's implementation.
+class Data
+{
+public :
+	// Reads one .plt grid (dimension checked against the config's n_agents,
+	// all states sharing dim and TotalDof) and uploads it to the current CUDA
+	// device.
+	virtual void load(const char* filename, int istate) = 0;
+
+	// Unloads all states.
+	virtual void clear() = 0;
+
+	virtual ~Data() { }
+};
+
+// Vector width hint of a device (LinearBasis/cuda/include/SIMDVector.h:10-38):
+// a warp, for 4- and 8-byte elements.
+class SIMDVector
+{
+	const Device* device;
+
+public :
+	explicit SIMDVector(const Device* d) : device(d) { }
+
+	virtual size_t getLength(size_t szelement) const;
+
+	virtual ~SIMDVector() { }
+};
+
+// LinearBasis/cuda/include/DeviceProperties.h:10-22
+class DeviceProperties
+{
+	SIMDVector simdVector;
+
+public :
+	explicit DeviceProperties(const Device* device) : simdVector(device) { }
+
+	virtual const SIMDVector* getSIMDVector() const { return &simdVector; }
+
+	virtual ~DeviceProperties() { }
+};
 
 class Interpolator
 {
@@ -81,9 +122,6 @@ extern "C" {
 SGI_PLUGIN_NAMESPACE::Interpolator* getInterpolator();
 
 // LinearBasis/cuda/src/Data.cu:1210-1213: a Data object for nstates states.
-// Its virtual load(filename, istate) reads one .plt grid (dimension checked
-// against the config's n_agents, all states sharing dim and TotalDof) and
-// uploads it to the current CUDA device; clear() unloads all states.
 SGI_PLUGIN_NAMESPACE::Data* getData(int nstates);
 
 // LinearBasis/cuda/src/supported.cpp:13-20: true if at least one GPU exists.
