@@ -916,3 +916,115 @@ extern "C" int sgi_backward(sgi_grid_t g, long long npts, const double* x, const
 	return SGI_OK;
 #undef BWD_TRY
 }
+
+// ------------------------------------------------- forward without allocation
+//
+// sgi_interpolate_noalloc: the work counters of its launches live in this
+// fixed array of the module's device image instead of the lazily allocated
+// per-device workspace.  Host code must not use the symbol itself as a device
+// address; it takes the address from cudaGetSymbolAddress once per device.
+
+static __device__ __align__(256) unsigned long long g_noalloc_counters[SGI_NOALLOC_MAX_LAUNCHES];
+
+namespace {
+
+std::mutex g_noalloc_mtx;
+std::vector<unsigned long long*> g_noalloc_addr; // per device; null until set up
+std::vector<int> g_noalloc_sms;
+
+// With `dev` current: the array's device address and the SM count, looked up
+// on the first call for this device.
+int noalloc_setup(int dev, unsigned long long** addr, int* sms)
+{
+	std::lock_guard<std::mutex> lk(g_noalloc_mtx);
+	if ((int)g_noalloc_addr.size() <= dev) { g_noalloc_addr.resize(dev + 1, nullptr); g_noalloc_sms.resize(dev + 1, 0); }
+	if (!g_noalloc_addr[dev])
+	{
+		unsigned long long* p = nullptr;
+		cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_counters);
+		if (e != cudaSuccess) return fail(SGI_E_CUDA, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+		int n = 0;
+		e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+		if (e != cudaSuccess) return fail(SGI_E_CUDA, "cudaDeviceGetAttribute failed: %s", cudaGetErrorString(e));
+		g_noalloc_sms[dev] = n;
+		g_noalloc_addr[dev] = p;
+	}
+	*addr = g_noalloc_addr[dev];
+	*sms = g_noalloc_sms[dev];
+	return SGI_OK;
+}
+
+} // namespace
+
+extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, int precision, void* stream_)
+{
+	clear_error();
+	int rc = check_set(ngrids, grids, pt_offsets);
+	if (rc) return rc;
+	if (pt_offsets[ngrids] > 0 && (!x || !out)) return fail(SGI_E_INVALID, "null x or out");
+	if (precision != SGI_FP64 && precision != SGI_FP32C) return fail(SGI_E_INVALID, "unknown precision %d", precision);
+	for (int k = 0; k < ngrids; k++)
+	{
+		if (precision == SGI_FP64 && !grids[k]->s64) return fail(SGI_E_INVALID, "grid %d has no FP64 surplus", k);
+		if (precision == SGI_FP32C && !grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k);
+	}
+	const sgi_grid* g0 = grids[0];
+	const size_t smem = (size_t)WARPS * g0->dim * sizeof(double);
+	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
+	// count the launches first: reject before launching anything
+	const int passes = (g0->TD + 32 * RMAX - 1) / (32 * RMAX);
+	long long launches = 0;
+	for (int gb = 0; gb < ngrids; gb += MAXG)
+		if (pt_offsets[std::min(ngrids, gb + MAXG)] > pt_offsets[gb]) launches += passes;
+	if (launches > SGI_NOALLOC_MAX_LAUNCHES)
+		return fail(SGI_E_RANGE, "call needs %lld kernel launches; the no-allocation scratch holds work counters "
+			"for at most %d (ceil(ngrids/%d) * ceil(TotalDof/%d) launches)", launches, SGI_NOALLOC_MAX_LAUNCHES,
+			MAXG, 32 * RMAX);
+	DeviceGuard guard(g0->device);
+	cudaStream_t stream = (cudaStream_t)stream_;
+	unsigned long long* counters = nullptr;
+	int sms = 0;
+	rc = noalloc_setup(g0->device, &counters, &sms);
+	if (rc) return rc;
+	g_stats = sgi_launch_stats{};
+	int slot = 0;
+	for (int gb = 0; gb < ngrids; gb += MAXG)
+	{
+		const int ng = std::min(MAXG, ngrids - gb);
+		const long long p0 = pt_offsets[gb], p1 = pt_offsets[gb + ng];
+		if (p1 == p0) continue;
+		FwdArgs a;
+		memset(&a, 0, sizeof(a));
+		for (int k = 0; k < ng; k++) a.g[k] = desc_of(grids[gb + k], pt_offsets[gb + k] - p0);
+		a.x = x + (size_t)p0 * g0->dim;
+		a.out = out + (size_t)p0 * g0->TD;
+		a.npts = p1 - p0;
+		a.ngrids = ng; a.dim = g0->dim; a.TD = g0->TD;
+		for (int ob = 0; ob < g0->TD; ob += 32 * RMAX)
+		{
+			a.o_begin = ob;
+			const int R = pick_R(std::min(g0->TD - ob, 32 * RMAX));
+			a.counter = counters + slot++;
+			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
+			void (*kern)(FwdArgs) = nullptr;
+			if (precision == SGI_FP64)
+				kern = R == 1 ? fwd_f64_kernel<1> : R == 2 ? fwd_f64_kernel<2> : R == 4 ? fwd_f64_kernel<4> : fwd_f64_kernel<8>;
+			else
+				kern = R == 1 ? fwd_f32c_kernel<1> : R == 2 ? fwd_f32c_kernel<2> : R == 4 ? fwd_f32c_kernel<4> : fwd_f32c_kernel<8>;
+			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			int blocks = 0;
+			rc = occupancy_grid(kern, smem, sms, &blocks);
+			if (rc) return rc;
+			const long long need = (a.npts + WARPS - 1) / WARPS;
+			if (blocks > need) blocks = (int)need;
+			kern<<<blocks, BLOCK, smem, stream>>>(a);
+			CUDA_TRY(cudaGetLastError());
+			g_stats.kernels++;
+			g_stats.grid_blocks = blocks;
+			g_stats.block_threads = BLOCK;
+		}
+		g_stats.points += a.npts;
+	}
+	return SGI_OK;
+}

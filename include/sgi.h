@@ -167,6 +167,34 @@ int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const long long* p
 int sgi_backward(sgi_grid_t g, long long npts, const double* x, const double* gout,
 	double* gx, double* gsurplus, void* stream);
 
+/* Forward without any device allocation.  No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory: a host solver that hands
+ * all device memory to its own pre-reserved arena (an extra cudaMalloc can
+ * fail or fragment it), code whose first call already runs inside CUDA stream
+ * capture (cudaMalloc is not permitted while a stream is capturing), and
+ * time-stepping loops that cannot afford cudaMalloc's implicit device
+ * synchronization.  sgi_interpolate's work counters live in a workspace that
+ * its first call on a device allocates; this variant instead keeps them in a
+ * fixed array inside the library's device image, SGI_NOALLOC_MAX_LAUNCHES
+ * counters of 8 bytes per device, held by every GPU that loads the library
+ * until the process exits.
+ *
+ * Arguments and results are those of sgi_interpolate (device x and out, host
+ * pt_offsets).  A call makes ceil(ngrids / 48) * ceil(TotalDof / 256) kernel
+ * launches (groups of grids with no points are skipped); a call that would need
+ * more than SGI_NOALLOC_MAX_LAUNCHES launches is rejected with SGI_E_RANGE
+ * before anything is launched.  The first call on each device looks up the
+ * array's device address with that device current; make that first call before
+ * any stream capture.  Every call shares the one array and clears the counters
+ * it uses on `stream` before each launch, so calls that overlap on the GPU
+ * (different streams, or different host threads) race on the counters and must
+ * be serialized by the caller.  The call allocates nothing, neither itself nor
+ * through CUDA or any library. */
+#define SGI_NOALLOC_MAX_LAUNCHES 64
+int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, int precision, void* stream);
+
 /* Active-node count A(x) per point (device int64 out[npts]); diagnostics. */
 int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream);
 

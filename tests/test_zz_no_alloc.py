@@ -1,0 +1,73 @@
+"""sgi_interpolate_noalloc: the forward pass for callers that must not allocate
+device memory (a solver whose device memory is all in its own arena, a first
+call made inside stream capture, a loop that cannot take cudaMalloc's implicit
+synchronization).  Its work counters live in a fixed array of the library's
+device image instead of a workspace allocated on first use.
+
+Checked through the C ABI against sgi_interpolate, the entry point that
+allocates its workspace, on two calls in a row (the shared counter array keeps
+the previous call's contents, so the second call shows it is cleared).  The
+FP64 form must match bit for bit, as every FP64 test here does; the FP32C form
+must match sgi_interpolate's FP32C bits and stay within 1e-7 of FP64.
+
+Named so that pytest collects it last."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import hddm_b200 as H
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+_fn = H.lib.sgi_interpolate_noalloc
+_fn.restype = ctypes.c_int
+_fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_int, ctypes.c_void_p]
+SGI_E_RANGE = -4
+MAX_LAUNCHES = 64
+
+
+def _noalloc(grids, x, counts, precision, out):
+    import torch
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    arr = (ctypes.c_void_p * len(grids))(*[g.handle.value for g in grids])
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return _fn(len(grids), arr, offs.ctypes.data, x.data_ptr(), out.data_ptr(), precision, stream)
+
+
+def test_noalloc_matches_allocating_entry_point(cuda):
+    import torch
+    hosts = [H.HostGrid.adaptive(30, n, 300, seed=40 + k) for k, n in enumerate((3000, 9000, 500, 6000))]
+    grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
+    counts = [700, 0, 13, 1500]
+    X = H.gen_points(30, sum(counts), kind=2, seed=12)
+    x = torch.from_numpy(X).cuda()
+    ref64 = H.interpolate(grids, x, counts=counts, precision=H.FP64).cpu().numpy()
+    ref32 = H.interpolate(grids, x, counts=counts, precision=H.FP32C).cpu().numpy()
+    for precision, ref in ((H.FP64, ref64), (H.FP32C, ref32)):
+        for call in range(2):
+            out = torch.full((x.shape[0], 300), float("nan"), dtype=torch.float64, device="cuda")
+            rc = _noalloc(grids, x, counts, precision, out)
+            assert rc == 0, H.lib.sgi_last_error().decode()
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            assert np.array_equal(got, ref), (precision, call)
+    assert O.rel_error(ref32, ref64)[0] <= 1e-7
+
+
+def test_noalloc_rejects_requests_beyond_its_scratch(cuda):
+    import torch
+    td = 256 * (MAX_LAUNCHES + 1)   # one launch per 256 outputs: 65 launches
+    idx = np.zeros((2, 4), np.int32)
+    idx[1, 0] = 2
+    hg = H.HostGrid.from_dense(idx, np.ones((2, td)))
+    g = H.Grid(hg)
+    x = torch.full((3, 2), 0.25, dtype=torch.float64, device="cuda")
+    out = torch.zeros((3, td), dtype=torch.float64, device="cuda")
+    rc = _noalloc([g], x, [3], H.FP64, out)
+    assert rc == SGI_E_RANGE
+    assert "at most 64" in H.lib.sgi_last_error().decode()
+    # the same grid through the allocating entry point works
+    assert float(H.interpolate(g, x).sum()) == pytest.approx(3 * td * 1.5)
