@@ -166,10 +166,20 @@ def run_gpu(args):
     perr = ((out32 - out64).abs() / den).amax(dim=1)
     err_max, err_rms = float(perr.max()), float(perr.pow(2).mean().sqrt())
     if args.only_accuracy_pass:
+        H.active_count(grid, x, stream=stream)
+        torch.cuda.synchronize(dev)
         print(json.dumps({"fp32c_max_rel_err": err_max, "fp32c_rms_rel_err": err_rms, "points": npts}))
         return
-    counts = H.active_count(grid, x[:65536], stream=stream).double()
-    mean_active = float(counts.mean())
+    # the tree walk alone (hit counting, no accumulation) over every point
+    for _ in range(2):
+        counts = H.active_count(grid, x, stream=stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    counts = H.active_count(grid, x, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    walk_ms = e0.elapsed_time(e1)
+    mean_active = float(counts.double().mean())
 
     with Clocks(local) as clk:
         t32, per32, k32 = timed(H.FP32C, out32, args.steps, args.warmup)
@@ -246,6 +256,7 @@ def run_gpu(args):
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                          "peak_kind": f"{peak_kind} (burst copy)", "algorithmic_bytes_per_launch": b32,
                          "traffic": traffic, "kernel": "fwd_f32c_kernel"},
+            "walk_only_ms": walk_ms,
             "fma_work": {"mean_active_nodes": mean_active,
                          "flops_per_launch": 2.0 * mean_active * TD * npts,
                          "achieved_tflops": 2.0 * mean_active * TD * npts / (ms32 * 1e-3) / 1e12},

@@ -42,7 +42,7 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int MAXG = 48;       // grids per launch (kernel parameter space)
 constexpr int BLOCK = 256;     // threads per block: 8 warps
 constexpr int WARPS = BLOCK / 32;
-constexpr int RMAX = 8;        // accumulator slots per lane: 256 outputs per pass
+constexpr int PASS = 256;      // outputs per launch pass (TotalDof > 256: several passes)
 
 struct GridDesc
 {
@@ -50,8 +50,9 @@ struct GridDesc
 	const uint2* comps;
 	const double* s64;
 	const float* s32;
-	const float* s32lo;
-	const uint32_t* lo_index;
+	const double* s64c;          // FP64 copies of the coarse rows (FP32C form)
+	const uint32_t* coarse_index; // row of node n in s64c, for coarse nodes
+	const int* parent;           // tree parent per node (-1 for roots)
 	long long pt_begin;
 	int nno;
 	int ld;
@@ -65,6 +66,9 @@ struct FwdArgs
 	unsigned long long* counter;
 	long long npts;
 	int ngrids, dim, TD, o_begin;
+	// node range of this launch: [chunk_begin, chunk_begin + chunk_len) of
+	// every grid; chunk_len 0 means the whole grid
+	int chunk_begin, chunk_len;
 };
 
 __device__ __forceinline__ double hat(double x, uint32_t ij)
@@ -80,27 +84,30 @@ __device__ __forceinline__ int find_grid(const FwdArgs& a, long long p)
 	return gi;
 }
 
-// Walks one grid for the point whose coordinates are in xs (shared memory).
-// Calls on_hits(mask, n0, w, rec) per window; bits of mask are hit lanes,
-// lane k's w is the weight of node n0+k and rec its record.
+// Walks nodes [a, b) of one grid for the point whose coordinates are in xs
+// (shared memory).  Calls on_hits(mask, n0, w, rec) per window; bits of mask
+// are hit lanes, lane k's w is the weight of node n0+k and rec its record.
+// A node whose tree parent lies before `a` ("chunk root") is checked on all its
+// components, since its ancestors are not walked; inside the range a node is
+// reached only when all its ancestors in the range are active.
 template <class OnHits>
-__device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, OnHits&& on_hits)
+__device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, int a, int b,
+	OnHits&& on_hits)
 {
-	int n0 = 0;
-	const int nno = G.nno;
-	while (n0 < nno)
+	int n0 = a;
+	while (n0 < b)
 	{
 		const int idx = n0 + lane;
-		const bool valid = idx < nno;
+		const bool valid = idx < b;
 		uint4 r = make_uint4(0u, 0u, 0u, 0u);
 		if (valid) r = __ldg(G.rec + idx);
 		const uint32_t ncomp = r.z & 0xffu;
+		const bool chunk_root = a > 0 && valid && __ldg(G.parent + idx) < a;
 		bool act = false;
 		if (valid)
 		{
 			if (r.z & NODE_DEAD) act = false;
-			else if (r.z & NODE_ALWAYS) act = true;
-			else if (r.z & NODE_MULTI)
+			else if ((r.z & NODE_MULTI) || chunk_root)
 			{
 				act = true;
 				for (uint32_t c = 0; c < ncomp && act; c++)
@@ -109,6 +116,7 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 					act = hat(xs[cp.x], cp.y) > 0.0;
 				}
 			}
+			else if (r.z & NODE_ALWAYS) act = true;
 			else act = hat(xs[r.z >> 16], r.w) > 0.0;
 		}
 		const unsigned cover = (valid && !act) ? r.x : 0u;
@@ -139,6 +147,19 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 	}
 }
 
+template <class OnHits>
+__device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, OnHits&& on_hits)
+{
+	traverse(G, xs, lane, 0, G.nno, on_hits);
+}
+
+// Node range of this launch for grid G.
+__device__ __forceinline__ void chunk_of(const FwdArgs& a, const GridDesc& G, int* lo, int* hi)
+{
+	*lo = a.chunk_begin;
+	*hi = a.chunk_len ? (int)min((long long)G.nno, (long long)a.chunk_begin + a.chunk_len) : G.nno;
+}
+
 // Loads point p into the warp's shared slot; returns false (after writing NaN
 // outputs, as the gold kernel produces for a non-finite coordinate) if any
 // coordinate is not finite.
@@ -155,12 +176,41 @@ __device__ __forceinline__ bool load_point(const FwdArgs& a, long long p, double
 	return __all_sync(FULL, finite);
 }
 
-template <int R>
+// Output ownership: with E = 2, lane l owns outputs 64v + 2l + {0, 1} of the
+// pass (v < V), so every row read is one coalesced 16-byte (FP64) or 8-byte
+// (FP32) load per lane; with E = 1 (TotalDof <= 32) lane l owns output l.
+template <int E>
+__device__ __forceinline__ int out_col(int v, int lane) { return v * 32 * E + lane * E; }
+
+template <int E>
+__device__ __forceinline__ void load_row(const double* row, int o, bool in, double* d)
+{
+	if (E == 2)
+	{
+		const double2 t = in ? __ldg(reinterpret_cast<const double2*>(row + o)) : make_double2(0.0, 0.0);
+		d[0] = t.x; d[1] = t.y;
+	}
+	else d[0] = in ? __ldg(row + o) : 0.0;
+}
+
+template <int E>
+__device__ __forceinline__ void load_row(const float* row, int o, bool in, float* d)
+{
+	if (E == 2)
+	{
+		const float2 t = in ? __ldg(reinterpret_cast<const float2*>(row + o)) : make_float2(0.f, 0.f);
+		d[0] = t.x; d[1] = t.y;
+	}
+	else d[0] = in ? __ldg(row + o) : 0.f;
+}
+
+template <int V, int E>
 __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ FwdArgs a)
 {
 	extern __shared__ double smem[];
 	const int lane = threadIdx.x & 31;
 	double* xs = smem + (threadIdx.x >> 5) * a.dim;
+	const bool first = a.chunk_begin == 0;
 	for (;;)
 	{
 		long long p = 0;
@@ -168,13 +218,26 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 		p = __shfl_sync(FULL, p, 0);
 		if (p >= a.npts) break;
 		const GridDesc& G = a.g[find_grid(a, p)];
-		double acc[R];
+		int lo, hi;
+		chunk_of(a, G, &lo, &hi);
+		if (!first && lo >= hi) continue;   // this grid has no nodes in the chunk
+		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
+		// the running sums continue from the previous chunk, so the adds keep
+		// the gold loop's order across chunks
+		double acc[V][E];
 #pragma unroll
-		for (int r = 0; r < R; r++) acc[r] = 0.0;
+		for (int v = 0; v < V; v++)
+#pragma unroll
+			for (int e = 0; e < E; e++)
+			{
+				const int o = out_col<E>(v, lane) + e;
+				acc[v][e] = (!first && a.o_begin + o < a.TD) ? __ldcs(dst + o) : 0.0;
+			}
 		const bool ok = load_point(a, p, xs, lane);
+		if (!ok && !first) continue;        // NaN already written by the first chunk
 		if (ok)
 		{
-			traverse(G, xs, lane, [&](unsigned mask, int n0, double w, const uint4&)
+			traverse(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&)
 			{
 				// two hits per step, both rows loaded before either is added, so
 				// that each warp keeps two rows in flight; the adds stay in order
@@ -189,46 +252,53 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 					const double w1 = __shfl_sync(FULL, w, k1);
 					const double* row0 = G.s64 + (size_t)(n0 + k0) * G.ld + a.o_begin;
 					const double* row1 = G.s64 + (size_t)(n0 + k1) * G.ld + a.o_begin;
-					double v0[R], v1[R];
+					double s0[V][E], s1[V][E];
 #pragma unroll
-					for (int r = 0; r < R; r++)
+					for (int v = 0; v < V; v++)
 					{
-						const int o = lane + 32 * r;
+						const int o = out_col<E>(v, lane);
 						const bool in = a.o_begin + o < G.ld;
-						v0[r] = in ? __ldg(row0 + o) : 0.0;
-						v1[r] = in && two ? __ldg(row1 + o) : 0.0;
+						load_row<E>(row0, o, in, s0[v]);
+						load_row<E>(row1, o, in && two, s1[v]);
 					}
 #pragma unroll
-					for (int r = 0; r < R; r++)
-					{
-						acc[r] = __dadd_rn(acc[r], __dmul_rn(w0, v0[r]));
-						if (two) acc[r] = __dadd_rn(acc[r], __dmul_rn(w1, v1[r]));
-					}
+					for (int v = 0; v < V; v++)
+#pragma unroll
+						for (int e = 0; e < E; e++)
+						{
+							acc[v][e] = __dadd_rn(acc[v][e], __dmul_rn(w0, s0[v][e]));
+							if (two) acc[v][e] = __dadd_rn(acc[v][e], __dmul_rn(w1, s1[v][e]));
+						}
 				}
 			});
 		}
-		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
 #pragma unroll
-		for (int r = 0; r < R; r++)
-		{
-			const int o = lane + 32 * r;
-			if (a.o_begin + o < a.TD) dst[o] = ok ? acc[r] : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0);
-		}
+		for (int v = 0; v < V; v++)
+#pragma unroll
+			for (int e = 0; e < E; e++)
+			{
+				const int o = out_col<E>(v, lane) + e;
+				if (a.o_begin + o < a.TD)
+					__stcs(dst + o, ok ? acc[v][e] : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0));
+			}
 		__syncwarp();
 	}
 }
 
-// FP32 + compensated form.  Per output: a double-float accumulator (hi, lo)
-// for coarse rows, whose terms are formed from the hi/lo splits of weight and
-// surplus with an exact FMA product error, added with TwoSum; a Kahan-
-// compensated FP32 accumulator for the other rows; the parts are summed in
-// FP64 at the end.
-template <int R>
+// FP32 + compensated form.  Rows are read in FP32, except the coarse rows
+// (largest |surplus| at least 2^-12 of the grid's largest), whose terms carry
+// most of the value and are read in FP64 and added with one FP64 FMA.  Other
+// hits are taken in pairs: each weight is split into FP32 hi and lo parts, the
+// pair's four FP32 products are summed in FP32 (the split keeps the weight's
+// rounding out of the result), and the pair sum is added to the output's FP64
+// running sum, which also carries the sums across node chunks.
+template <int V, int E>
 __global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__ FwdArgs a)
 {
 	extern __shared__ double smem[];
 	const int lane = threadIdx.x & 31;
 	double* xs = smem + (threadIdx.x >> 5) * a.dim;
+	const bool first = a.chunk_begin == 0;
 	for (;;)
 	{
 		long long p = 0;
@@ -236,83 +306,92 @@ __global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__
 		p = __shfl_sync(FULL, p, 0);
 		if (p >= a.npts) break;
 		const GridDesc& G = a.g[find_grid(a, p)];
-		float ch[R], cl[R], fa[R], fc[R];
+		int lo_n, hi_n;
+		chunk_of(a, G, &lo_n, &hi_n);
+		if (!first && lo_n >= hi_n) continue;   // this grid has no nodes in the chunk
+		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
+		double acc[V][E];
 #pragma unroll
-		for (int r = 0; r < R; r++) { ch[r] = 0.f; cl[r] = 0.f; fa[r] = 0.f; fc[r] = 0.f; }
+		for (int v = 0; v < V; v++)
+#pragma unroll
+			for (int e = 0; e < E; e++)
+			{
+				const int o = out_col<E>(v, lane) + e;
+				acc[v][e] = (!first && a.o_begin + o < a.TD) ? __ldcs(dst + o) : 0.0;
+			}
 		const bool ok = load_point(a, p, xs, lane);
+		if (!ok && !first) continue;            // NaN already written by the first chunk
 		if (ok)
 		{
-			traverse(G, xs, lane, [&](unsigned mask, int n0, double w, const uint4& rec)
+			traverse(G, xs, lane, lo_n, hi_n, [&](unsigned mask, int n0, double w, const uint4& rec)
 			{
-				uint32_t lo = 0u;
-				if ((mask >> lane) & 1u)
-					if (rec.z & NODE_COARSE) lo = __ldg(G.lo_index + n0 + lane);
-				while (mask)
+				const bool mine = (mask >> lane) & 1u;
+				unsigned cm = __ballot_sync(FULL, mine && (rec.z & NODE_COARSE));
+				const uint32_t ci = ((cm >> lane) & 1u) ? __ldg(G.coarse_index + n0 + lane) : 0u;
+				unsigned fm = mask & ~cm;
+				while (cm)
 				{
-					const int k = __ffs(mask) - 1;
-					mask &= mask - 1;
+					const int k = __ffs(cm) - 1;
+					cm &= cm - 1;
 					const double wk = __shfl_sync(FULL, w, k);
-					const uint32_t zk = __shfl_sync(FULL, rec.z, k);
-					const uint32_t lok = __shfl_sync(FULL, lo, k);
-					const float whi = __double2float_rn(wk);
-					const float* row = G.s32 + (size_t)(n0 + k) * G.ld + a.o_begin;
-					if (zk & NODE_COARSE)
+					const double* row = G.s64c + (size_t)__shfl_sync(FULL, ci, k) * G.ld + a.o_begin;
+					double sv[V][E];
+#pragma unroll
+					for (int v = 0; v < V; v++)
 					{
-						const float wlo = __double2float_rn(wk - (double)whi);
-						const float* rlo = G.s32lo + (size_t)lok * G.ld + a.o_begin;
-						float shi[R], slo[R];
-#pragma unroll
-						for (int r = 0; r < R; r++)
-						{
-							const int o = lane + 32 * r;
-							const bool in = a.o_begin + o < G.ld;
-							shi[r] = in ? __ldg(row + o) : 0.f;
-							slo[r] = in ? __ldg(rlo + o) : 0.f;
-						}
-#pragma unroll
-						for (int r = 0; r < R; r++)
-						{
-							const float pr = __fmul_rn(whi, shi[r]);
-							const float pe = __fmaf_rn(whi, shi[r], -pr);
-							const float tl = __fmaf_rn(whi, slo[r], __fmaf_rn(wlo, shi[r], pe));
-							const float s = __fadd_rn(ch[r], pr);
-							const float bp = __fsub_rn(s, ch[r]);
-							const float e = __fadd_rn(__fsub_rn(ch[r], __fsub_rn(s, bp)), __fsub_rn(pr, bp));
-							ch[r] = s;
-							cl[r] = __fadd_rn(cl[r], __fadd_rn(e, tl));
-						}
+						const int o = out_col<E>(v, lane);
+						load_row<E>(row, o, a.o_begin + o < G.ld, sv[v]);
 					}
-					else
+#pragma unroll
+					for (int v = 0; v < V; v++)
+#pragma unroll
+						for (int e = 0; e < E; e++) acc[v][e] = fma(wk, sv[v][e], acc[v][e]);
+				}
+				while (fm)
+				{
+					const int k0 = __ffs(fm) - 1;
+					fm &= fm - 1;
+					const bool two = fm != 0u;
+					const int k1 = two ? __ffs(fm) - 1 : k0;
+					if (two) fm &= fm - 1;
+					const double w0 = __shfl_sync(FULL, w, k0);
+					const double w1 = two ? __shfl_sync(FULL, w, k1) : 0.0;
+					const float w0h = __double2float_rn(w0), w0l = __double2float_rn(w0 - (double)w0h);
+					const float w1h = __double2float_rn(w1), w1l = __double2float_rn(w1 - (double)w1h);
+					const float* row0 = G.s32 + (size_t)(n0 + k0) * G.ld + a.o_begin;
+					const float* row1 = G.s32 + (size_t)(n0 + k1) * G.ld + a.o_begin;
+					float s0[V][E], s1[V][E];
+#pragma unroll
+					for (int v = 0; v < V; v++)
 					{
-						float sv[R];
-#pragma unroll
-						for (int r = 0; r < R; r++)
-						{
-							const int o = lane + 32 * r;
-							sv[r] = a.o_begin + o < G.ld ? __ldg(row + o) : 0.f;
-						}
-#pragma unroll
-						for (int r = 0; r < R; r++)
-						{
-							const float t = __fmul_rn(whi, sv[r]);
-							const float y = __fsub_rn(t, fc[r]);
-							const float s = __fadd_rn(fa[r], y);
-							fc[r] = __fsub_rn(__fsub_rn(s, fa[r]), y);
-							fa[r] = s;
-						}
+						const int o = out_col<E>(v, lane);
+						const bool in = a.o_begin + o < G.ld;
+						load_row<E>(row0, o, in, s0[v]);
+						load_row<E>(row1, o, in, s1[v]);
 					}
+#pragma unroll
+					for (int v = 0; v < V; v++)
+#pragma unroll
+						for (int e = 0; e < E; e++)
+						{
+							float f = __fmul_rn(w0l, s0[v][e]);
+							f = __fmaf_rn(w1l, s1[v][e], f);
+							f = __fmaf_rn(w1h, s1[v][e], f);
+							f = __fmaf_rn(w0h, s0[v][e], f);
+							acc[v][e] = __dadd_rn(acc[v][e], (double)f);
+						}
 				}
 			});
 		}
-		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
 #pragma unroll
-		for (int r = 0; r < R; r++)
-		{
-			const int o = lane + 32 * r;
-			if (a.o_begin + o < a.TD)
-				dst[o] = ok ? (((double)ch[r] + (double)cl[r]) + ((double)fa[r] - (double)fc[r]))
-				            : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0);
-		}
+		for (int v = 0; v < V; v++)
+#pragma unroll
+			for (int e = 0; e < E; e++)
+			{
+				const int o = out_col<E>(v, lane) + e;
+				if (a.o_begin + o < a.TD)
+					__stcs(dst + o, ok ? acc[v][e] : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0));
+			}
 		__syncwarp();
 	}
 }
@@ -501,6 +580,7 @@ struct DeviceWork
 	unsigned long long* counters = nullptr;
 	std::atomic<unsigned> next{0};
 	int sms = 0;
+	int l2_bytes = 0;
 	// host-pointer staging
 	double* dx = nullptr; size_t dx_bytes = 0;
 	double* dout = nullptr; size_t dout_bytes = 0;
@@ -520,10 +600,32 @@ int device_work(int dev, DeviceWork** out)
 		DeviceWork* w = new DeviceWork;
 		CUDA_TRY(cudaMalloc(&w->counters, sizeof(unsigned long long) * NCOUNTERS));
 		CUDA_TRY(cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, dev));
+		CUDA_TRY(cudaDeviceGetAttribute(&w->l2_bytes, cudaDevAttrL2CacheSize, dev));
 		g_work[dev] = w;
 	}
 	*out = g_work[dev];
 	return SGI_OK;
+}
+
+// Node-range chunk for the forward launches: grids whose surplus rows exceed
+// half the L2 are walked in node ranges whose rows fit in that half, all
+// points per range, so that the rows each range gathers stay L2-resident.
+// Small batches are not chunked.  sgi_set_chunk_rows (or SGI_CHUNK_ROWS at
+// start-up) overrides: 0 = no chunks, n > 0 = chunks of n nodes.
+std::atomic<int> g_chunk_override{[]() { const char* e = getenv("SGI_CHUNK_ROWS"); return e ? atoi(e) : -1; }()};
+
+int chunk_rows_env() { return g_chunk_override.load(); }
+
+// Forward kernel for a pass of `cols` outputs with row stride ld.
+void (*select_fwd(int precision, int ld, int cols))(FwdArgs)
+{
+	if (ld <= 32)
+		return precision == SGI_FP64 ? fwd_f64_kernel<1, 1> : fwd_f32c_kernel<1, 1>;
+	if (cols <= 64)
+		return precision == SGI_FP64 ? fwd_f64_kernel<1, 2> : fwd_f32c_kernel<1, 2>;
+	if (cols <= 128)
+		return precision == SGI_FP64 ? fwd_f64_kernel<2, 2> : fwd_f32c_kernel<2, 2>;
+	return precision == SGI_FP64 ? fwd_f64_kernel<4, 2> : fwd_f32c_kernel<4, 2>;
 }
 
 int pick_R(int cols)
@@ -533,6 +635,8 @@ int pick_R(int cols)
 	if (cols <= 128) return 4;
 	return 8;
 }
+
+int chunk_rows(const DeviceWork* W, const sgi_grid* g0, int precision, long long npts, int maxnno);
 
 template <class K>
 int occupancy_grid(K kernel, size_t smem, int sms, int* blocks)
@@ -556,12 +660,23 @@ struct sgi_grid
 	uint2* comps = nullptr;
 	double* s64 = nullptr;
 	float* s32 = nullptr;
-	float* s32lo = nullptr;
-	uint32_t* lo_index = nullptr;
+	double* s64c = nullptr;
+	uint32_t* coarse_index = nullptr;
+	int* parent = nullptr;
 	sgi_grid_info info{};
 };
 
 namespace {
+
+int chunk_rows(const DeviceWork* W, const sgi_grid* g0, int precision, long long npts, int maxnno)
+{
+	const int env = chunk_rows_env();
+	if (env >= 0) return env >= maxnno ? 0 : env;
+	const long long row = (long long)g0->ld * (precision == SGI_FP64 ? 8 : 4);
+	const long long rows = std::max(1024ll, (long long)W->l2_bytes / 2 / row);
+	if (npts < 4096 || maxnno <= rows) return 0;
+	return (int)rows;
+}
 
 void free_grid(sgi_grid* g)
 {
@@ -569,7 +684,8 @@ void free_grid(sgi_grid* g)
 	int prev = 0;
 	cudaGetDevice(&prev);
 	cudaSetDevice(g->device);
-	cudaFree(g->rec); cudaFree(g->comps); cudaFree(g->s64); cudaFree(g->s32); cudaFree(g->s32lo); cudaFree(g->lo_index);
+	cudaFree(g->rec); cudaFree(g->comps); cudaFree(g->s64); cudaFree(g->s32); cudaFree(g->s64c); cudaFree(g->coarse_index);
+	cudaFree(g->parent);
 	cudaSetDevice(prev);
 	delete g;
 }
@@ -577,8 +693,8 @@ void free_grid(sgi_grid* g)
 GridDesc desc_of(const sgi_grid* g, long long pt_begin)
 {
 	GridDesc d;
-	d.rec = g->rec; d.comps = g->comps; d.s64 = g->s64; d.s32 = g->s32; d.s32lo = g->s32lo;
-	d.lo_index = g->lo_index; d.pt_begin = pt_begin; d.nno = g->nno; d.ld = g->ld;
+	d.rec = g->rec; d.comps = g->comps; d.s64 = g->s64; d.s32 = g->s32; d.s64c = g->s64c;
+	d.coarse_index = g->coarse_index; d.parent = g->parent; d.pt_begin = pt_begin; d.nno = g->nno; d.ld = g->ld;
 	return d;
 }
 
@@ -614,7 +730,9 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 	DeviceGuard guard(device);
 	sgi_grid* d = new sgi_grid;
 	d->device = device; d->dim = g.dim; d->nno = g.nno; d->TD = g.TotalDof;
-	d->ld = (g.TotalDof + 31) / 32 * 32;
+	// row stride: 32 for TotalDof <= 32 (a lane per output), else a multiple
+	// of 64 (a lane per output pair per 64 columns)
+	d->ld = g.TotalDof <= 32 ? 32 : (g.TotalDof + 63) / 64 * 64;
 	const size_t nrow = (size_t)std::max(g.nno, 1);
 	long long bytes = 0;
 	auto upload = [&](void** dst, const void* src, size_t n) -> int
@@ -631,7 +749,8 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 	};
 	rc = upload((void**)&d->rec, L.rec.data(), L.rec.size() * 4);
 	if (!rc) rc = upload((void**)&d->comps, L.comps.data(), L.comps.size() * 4);
-	if (!rc) rc = upload((void**)&d->lo_index, L.lo_index.data(), L.lo_index.size() * 4);
+	if (!rc) rc = upload((void**)&d->coarse_index, L.lo_index.data(), L.lo_index.size() * 4);
+	if (!rc) rc = upload((void**)&d->parent, L.parent.data(), L.parent.size() * 4);
 	if (!rc && !(flags & SGI_BUILD_NO_FP64))
 	{
 		std::vector<double> s(nrow * d->ld, 0.0);
@@ -641,17 +760,17 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 	}
 	if (!rc && (flags & (SGI_BUILD_FP32 | SGI_BUILD_NO_FP64)))
 	{
-		std::vector<float> hi(nrow * d->ld, 0.f), lo((size_t)std::max(L.ncoarse, 1) * d->ld, 0.f);
+		std::vector<float> hi(nrow * d->ld, 0.f);
+		std::vector<double> coarse((size_t)std::max(L.ncoarse, 1) * d->ld, 0.0);
 		for (int n = 0; n < g.nno; n++)
 			for (int o = 0; o < g.TotalDof; o++)
 			{
 				const double v = g.surplus[(size_t)n * g.TotalDof + o];
-				const float h = (float)v;
-				hi[(size_t)n * d->ld + o] = h;
-				if (L.lo_index[n] != ~0u) lo[(size_t)L.lo_index[n] * d->ld + o] = (float)(v - (double)h);
+				hi[(size_t)n * d->ld + o] = (float)v;
+				if (L.lo_index[n] != ~0u) coarse[(size_t)L.lo_index[n] * d->ld + o] = v;
 			}
 		rc = upload((void**)&d->s32, hi.data(), hi.size() * 4);
-		if (!rc) rc = upload((void**)&d->s32lo, lo.data(), lo.size() * 4);
+		if (!rc) rc = upload((void**)&d->s64c, coarse.data(), coarse.size() * 8);
 	}
 	if (rc) { free_grid(d); return rc; }
 	sgi_grid_info& I = d->info;
@@ -672,6 +791,13 @@ extern "C" int sgi_grid_info_get(sgi_grid_t g, sgi_grid_info* info)
 }
 
 extern "C" void sgi_grid_destroy(sgi_grid_t g) { free_grid(g); }
+
+extern "C" int sgi_set_chunk_rows(int rows)
+{
+	const int prev = g_chunk_override.load();
+	g_chunk_override.store(rows < 0 ? -1 : rows);
+	return prev;
+}
 
 extern "C" int sgi_last_launch(sgi_launch_stats* s)
 {
@@ -724,17 +850,19 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 		a.out = out + (size_t)p0 * g0->TD;
 		a.npts = p1 - p0;
 		a.ngrids = ng; a.dim = g0->dim; a.TD = g0->TD;
-		for (int ob = 0; ob < g0->TD; ob += 32 * RMAX)
+		int maxnno = 0;
+		for (int k = 0; k < ng; k++) maxnno = std::max(maxnno, grids[gb + k]->nno);
+		const int clen = chunk_rows(W, g0, precision, a.npts, maxnno);
+		const int nchunks = clen ? (maxnno + clen - 1) / clen : 1;
+		for (int ob = 0; ob < g0->TD; ob += PASS)
+		for (int c = 0; c < std::max(nchunks, 1); c++)
 		{
 			a.o_begin = ob;
-			const int R = pick_R(std::min(g0->TD - ob, 32 * RMAX));
+			a.chunk_begin = c * clen;
+			a.chunk_len = clen;
 			a.counter = W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = nullptr;
-			if (precision == SGI_FP64)
-				kern = R == 1 ? fwd_f64_kernel<1> : R == 2 ? fwd_f64_kernel<2> : R == 4 ? fwd_f64_kernel<4> : fwd_f64_kernel<8>;
-			else
-				kern = R == 1 ? fwd_f32c_kernel<1> : R == 2 ? fwd_f32c_kernel<2> : R == 4 ? fwd_f32c_kernel<4> : fwd_f32c_kernel<8>;
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS));
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, W->sms, &blocks);
@@ -824,7 +952,7 @@ extern "C" int sgi_backward(sgi_grid_t g, long long npts, const double* x, const
 	clear_error();
 	if (!g || npts < 0 || (npts && (!x || !gout))) return fail(SGI_E_INVALID, "bad arguments");
 	if (!g->s64) return fail(SGI_E_INVALID, "grid has no FP64 surplus");
-	if (g->TD > 32 * RMAX) return fail(SGI_E_RANGE, "backward supports TotalDof <= %d", 32 * RMAX);
+	if (g->TD > 256) return fail(SGI_E_RANGE, "backward supports TotalDof <= 256");
 	if (npts > 0xffffffffll) return fail(SGI_E_RANGE, "too many points");
 	cudaStream_t stream = (cudaStream_t)stream_;
 	DeviceGuard guard(g->device);
@@ -973,14 +1101,14 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 	const size_t smem = (size_t)WARPS * g0->dim * sizeof(double);
 	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	// count the launches first: reject before launching anything
-	const int passes = (g0->TD + 32 * RMAX - 1) / (32 * RMAX);
+	const int passes = (g0->TD + PASS - 1) / PASS;
 	long long launches = 0;
 	for (int gb = 0; gb < ngrids; gb += MAXG)
 		if (pt_offsets[std::min(ngrids, gb + MAXG)] > pt_offsets[gb]) launches += passes;
 	if (launches > SGI_NOALLOC_MAX_LAUNCHES)
 		return fail(SGI_E_RANGE, "call needs %lld kernel launches; the no-allocation scratch holds work counters "
 			"for at most %d (ceil(ngrids/%d) * ceil(TotalDof/%d) launches)", launches, SGI_NOALLOC_MAX_LAUNCHES,
-			MAXG, 32 * RMAX);
+			MAXG, PASS);
 	DeviceGuard guard(g0->device);
 	cudaStream_t stream = (cudaStream_t)stream_;
 	unsigned long long* counters = nullptr;
@@ -1001,17 +1129,12 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		a.out = out + (size_t)p0 * g0->TD;
 		a.npts = p1 - p0;
 		a.ngrids = ng; a.dim = g0->dim; a.TD = g0->TD;
-		for (int ob = 0; ob < g0->TD; ob += 32 * RMAX)
+		for (int ob = 0; ob < g0->TD; ob += PASS)
 		{
 			a.o_begin = ob;
-			const int R = pick_R(std::min(g0->TD - ob, 32 * RMAX));
 			a.counter = counters + slot++;
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = nullptr;
-			if (precision == SGI_FP64)
-				kern = R == 1 ? fwd_f64_kernel<1> : R == 2 ? fwd_f64_kernel<2> : R == 4 ? fwd_f64_kernel<4> : fwd_f64_kernel<8>;
-			else
-				kern = R == 1 ? fwd_f32c_kernel<1> : R == 2 ? fwd_f32c_kernel<2> : R == 4 ? fwd_f32c_kernel<4> : fwd_f32c_kernel<8>;
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS));
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, sms, &blocks);

@@ -73,6 +73,7 @@ def _load():
         "sgi_backward": (I, [P, LL, P, P, P, P, P]),
         "sgi_active_count": (I, [P, LL, P, P, P]),
         "sgi_last_launch": (I, [ctypes.POINTER(LaunchStats)]),
+        "sgi_set_chunk_rows": (I, [I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -304,6 +305,11 @@ def backward(grid, x, gout, want_x=True, want_surplus=True, stream=None):
                             gx.data_ptr() if gx is not None else None,
                             gs.data_ptr() if gs is not None else None, _stream_ptr(stream)))
     return gx, gs
+
+
+def set_chunk_rows(rows):
+    """-1 automatic, 0 never chunk, n > 0 chunks of n nodes; returns the previous setting."""
+    return lib.sgi_set_chunk_rows(rows)
 
 
 def last_launch():

@@ -183,3 +183,24 @@ def test_errors(cuda):
     with pytest.raises(H.SgiError) as e:
         H.interpolate(a, x, precision=H.FP32C)   # built without BUILD_FP32
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("rows", [37, 1000, 4096])
+def test_chunked_walk_bit_exact(cuda, rows):
+    """Node-range chunks (outputs carried across launches in FP64) keep gold's bits."""
+    hosts = [H.HostGrid.adaptive(59, 12000, 64, seed=30), H.HostGrid.adaptive(59, 3000, 64, seed=31)]
+    grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
+    counts = [300, 200]
+    X = H.gen_points(59, 500, kind=2, seed=33)
+    prev = H.set_chunk_rows(rows)
+    try:
+        out = _run(grids, X, counts=counts)
+        out32 = _run(grids, X, H.FP32C, counts=counts)
+        n = H.last_launch().kernels
+    finally:
+        H.set_chunk_rows(prev)
+    assert n == -(-12000 // rows)
+    for k, (h, sl) in enumerate(zip(hosts, (slice(0, 300), slice(300, 500)))):
+        ref = O.Gold(*h.arrays()).interpolate(X[sl])
+        assert np.array_equal(out[sl], ref), k
+        assert O.rel_error(out32[sl], ref)[0] <= FP32C_TOL, k
