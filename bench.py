@@ -143,20 +143,20 @@ def run_gpu(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def timed(precision, out, steps, warmup):
+    def timed(plan, steps, warmup):
+        """Replays of the plan's CUDA graph (autotuned node chunks)."""
         for _ in range(warmup):
-            H.interpolate(grid, x, precision=precision, out=out, stream=stream)
+            plan.launch(stream=stream)
         barrier()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
         ev[0].record(stream)
         for s in range(steps):
-            H.interpolate(grid, x, precision=precision, out=out, stream=stream)
+            plan.launch(stream=stream)
             ev[s + 1].record(stream)
         barrier()
         per = [ev[s].elapsed_time(ev[s + 1]) for s in range(steps)]
         total = ev[0].elapsed_time(ev[steps])
-        kernels = H.last_launch().kernels
-        return total, per, kernels
+        return total, per, plan.launches
 
     # accuracy of the FP32C form against the FP64 form (bit-identical to gold), all points
     H.interpolate(grid, x, precision=H.FP64, out=out64, stream=stream)
@@ -181,9 +181,13 @@ def run_gpu(args):
     walk_ms = e0.elapsed_time(e1)
     mean_active = float(counts.double().mean())
 
+    t_tune = time.time()
+    plan32 = H.Plan(grid, x, out32, precision=H.FP32C, chunk_rows=args.chunk_rows, stream=stream)
+    plan64 = H.Plan(grid, x, out64, precision=H.FP64, chunk_rows=args.chunk_rows, stream=stream)
+    t_tune = time.time() - t_tune
     with Clocks(local) as clk:
-        t32, per32, k32 = timed(H.FP32C, out32, args.steps, args.warmup)
-        t64, per64, k64 = timed(H.FP64, out64, args.steps, args.warmup)
+        t32, per32, k32 = timed(plan32, args.steps, args.warmup)
+        t64, per64, k64 = timed(plan64, args.steps, args.warmup)
     clocks = clk.summary()
 
     # end to end through the C ABI's host-pointer entry: pinned x in, pinned out back
@@ -264,7 +268,11 @@ def run_gpu(args):
                     "h2d_bytes_per_step": npts * DIM * 8, "d2h_bytes_per_step": npts * TD * 8},
             "gpu_launches": args.steps * (k32 + k64),
             "clocks": clocks,
-            "setup_s": {"generate": round(t_gen, 2), "layout_and_upload": round(t_upload, 2)},
+            "setup_s": {"generate": round(t_gen, 2), "layout_and_upload": round(t_upload, 2),
+                        "autotune_and_capture": round(t_tune, 2)},
+            "plans": {"fp32c": {"chunk_rows": plan32.chunk_rows, "launches": plan32.launches},
+                      "fp64": {"chunk_rows": plan64.chunk_rows, "launches": plan64.launches},
+                      "note": "each step replays one CUDA graph holding all node-chunk launches"},
         }
     if rank == 0 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(hg, X, args.cpu_sample, args.cpu_variant)
@@ -349,6 +357,7 @@ def main():
     ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=NPTS, help="points per GPU (default: the workload's 1M)")
+    ap.add_argument("--chunk-rows", type=int, default=-1, help="node-chunk size of the plans (-1: autotune)")
     ap.add_argument("--only-accuracy-pass", action="store_true",
                     help="run one FP64 and one FP32C launch, print their agreement and exit (profiling case)")
     args = ap.parse_args()

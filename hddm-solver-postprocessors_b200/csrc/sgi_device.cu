@@ -29,7 +29,9 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "sgi_internal.h"
@@ -825,8 +827,12 @@ int check_set(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets)
 	return SGI_OK;
 }
 
+// Launches of one forward call.  chunk < 0: the automatic chunk size; work
+// counters come from `counters` (one per launch, in order) when given, else
+// from the device workspace's ring.
 int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets, const double* x,
-	double* out, int precision, cudaStream_t stream)
+	double* out, int precision, cudaStream_t stream, int chunk = -1, unsigned long long* counters = nullptr,
+	int* nlaunch = nullptr)
 {
 	const sgi_grid* g0 = grids[0];
 	DeviceWork* W = nullptr;
@@ -838,6 +844,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 	const size_t smem = (size_t)WARPS * g0->dim * sizeof(double);
 	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	g_stats = sgi_launch_stats{};
+	int launches = 0;
 	for (int gb = 0; gb < ngrids; gb += MAXG)
 	{
 		const int ng = std::min(MAXG, ngrids - gb);
@@ -852,7 +859,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 		a.ngrids = ng; a.dim = g0->dim; a.TD = g0->TD;
 		int maxnno = 0;
 		for (int k = 0; k < ng; k++) maxnno = std::max(maxnno, grids[gb + k]->nno);
-		const int clen = chunk_rows(W, g0, precision, a.npts, maxnno);
+		const int clen = chunk < 0 ? chunk_rows(W, g0, precision, a.npts, maxnno) : (chunk >= maxnno ? 0 : chunk);
 		const int nchunks = clen ? (maxnno + clen - 1) / clen : 1;
 		for (int ob = 0; ob < g0->TD; ob += PASS)
 		for (int c = 0; c < std::max(nchunks, 1); c++)
@@ -860,7 +867,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 			a.o_begin = ob;
 			a.chunk_begin = c * clen;
 			a.chunk_len = clen;
-			a.counter = W->counters + (W->next.fetch_add(1) % NCOUNTERS);
+			a.counter = counters ? counters + launches : W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
 			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS));
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -871,13 +878,32 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 			if (blocks > need) blocks = (int)need;
 			kern<<<blocks, BLOCK, smem, stream>>>(a);
 			CUDA_TRY(cudaGetLastError());
+			launches++;
 			g_stats.kernels++;
 			g_stats.grid_blocks = blocks;
 			g_stats.block_threads = BLOCK;
 		}
 		g_stats.points += a.npts;
 	}
+	if (nlaunch) *nlaunch = launches;
 	return SGI_OK;
+}
+
+// Launch count of a forward call with chunk size `chunk` (as launch_forward).
+int count_launches(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets, int chunk)
+{
+	int n = 0;
+	const int passes = (grids[0]->TD + PASS - 1) / PASS;
+	for (int gb = 0; gb < ngrids; gb += MAXG)
+	{
+		const int ng = std::min(MAXG, ngrids - gb);
+		if (pt_offsets[gb + ng] == pt_offsets[gb]) continue;
+		int maxnno = 0;
+		for (int k = 0; k < ng; k++) maxnno = std::max(maxnno, grids[gb + k]->nno);
+		const int clen = chunk >= maxnno ? 0 : chunk;
+		n += passes * (clen ? (maxnno + clen - 1) / clen : 1);
+	}
+	return n;
 }
 
 } // namespace
@@ -1150,4 +1176,173 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		g_stats.points += a.npts;
 	}
 	return SGI_OK;
+}
+
+// ------------------------------------------------------- plans (CUDA graphs)
+//
+// A plan records every launch of one forward call (work-counter clears and
+// chunk launches) into a CUDA graph once and replays it with one
+// cudaGraphLaunch.  The chunk size is chosen by timing candidates on the
+// caller's own inputs the first time a (dim, largest nno, TotalDof,
+// precision, batch size) key is seen.
+
+struct sgi_plan
+{
+	int device = 0;
+	int chunk = 0;
+	int launches = 0;
+	unsigned long long* counters = nullptr;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	float tuned_ms = 0.f;
+};
+
+namespace {
+
+struct TuneKey
+{
+	int dim, maxnno, TD, precision;
+	long long npts;
+	bool operator<(const TuneKey& o) const
+	{
+		return std::tie(dim, maxnno, TD, precision, npts) < std::tie(o.dim, o.maxnno, o.TD, o.precision, o.npts);
+	}
+};
+std::mutex g_tune_mtx;
+std::map<TuneKey, std::pair<int, float>> g_tune;
+
+int time_forward(int ngrids, const sgi_grid_t* grids, const long long* offs, const double* x, double* out,
+	int precision, cudaStream_t s, int chunk, float* ms)
+{
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	CUDA_TRY(cudaEventCreate(&e0));
+	CUDA_TRY(cudaEventCreate(&e1));
+	int rc = launch_forward(ngrids, grids, offs, x, out, precision, s, chunk);
+	if (!rc) { cudaEventRecord(e0, s); rc = launch_forward(ngrids, grids, offs, x, out, precision, s, chunk); }
+	if (!rc) { cudaEventRecord(e1, s); cudaEventSynchronize(e1); cudaEventElapsedTime(ms, e0, e1); }
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	return rc;
+}
+
+void free_plan(sgi_plan* p)
+{
+	if (!p) return;
+	if (p->exec) cudaGraphExecDestroy(p->exec);
+	if (p->graph) cudaGraphDestroy(p->graph);
+	if (p->counters) cudaFree(p->counters);
+	delete p;
+}
+
+} // namespace
+
+extern "C" int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, int precision, int chunk_rows_req, void* stream_, sgi_plan_t* out_plan)
+{
+	clear_error();
+	if (!out_plan) return fail(SGI_E_INVALID, "null plan");
+	*out_plan = nullptr;
+	int rc = check_set(ngrids, grids, pt_offsets);
+	if (rc) return rc;
+	const long long npts = pt_offsets[ngrids];
+	if (npts > 0 && (!x || !out)) return fail(SGI_E_INVALID, "null x or out");
+	if (precision != SGI_FP64 && precision != SGI_FP32C) return fail(SGI_E_INVALID, "unknown precision %d", precision);
+	DeviceGuard guard(grids[0]->device);
+	cudaStream_t stream = (cudaStream_t)stream_;
+	DeviceWork* W = nullptr;
+	rc = device_work(grids[0]->device, &W);
+	if (rc) return rc;
+	int maxnno = 0;
+	for (int k = 0; k < ngrids; k++) maxnno = std::max(maxnno, grids[k]->nno);
+	sgi_plan* p = new sgi_plan;
+	p->device = grids[0]->device;
+	float tuned = 0.f;
+	int chunk = chunk_rows_req;
+	if (chunk < 0)
+	{
+		const TuneKey key{ grids[0]->dim, maxnno, grids[0]->TD, precision, npts };
+		bool hit = false;
+		{
+			std::lock_guard<std::mutex> lk(g_tune_mtx);
+			auto it = g_tune.find(key);
+			if (it != g_tune.end()) { chunk = it->second.first; tuned = it->second.second; hit = true; }
+		}
+		if (!hit)
+		{
+			// candidates: no chunks, and chunks whose rows fill 1/4 .. 2 x the L2
+			const long long row = (long long)grids[0]->ld * (precision == SGI_FP64 ? 8 : 4);
+			std::vector<int> cand{ 0 };
+			for (double f : { 0.25, 0.5, 1.0, 2.0 })
+			{
+				const long long r = std::max(1024ll, (long long)(W->l2_bytes * f / row));
+				if (r < maxnno) cand.push_back((int)r);
+			}
+			float best = 0.f;
+			int best_c = 0;
+			for (size_t q = 0; q < cand.size(); q++)
+			{
+				float ms = 0.f;
+				rc = time_forward(ngrids, grids, pt_offsets, x, out, precision, stream, cand[q], &ms);
+				if (rc) { free_plan(p); return rc; }
+				if (q == 0 || ms < best) { best = ms; best_c = cand[q]; }
+			}
+			chunk = best_c;
+			tuned = best;
+			std::lock_guard<std::mutex> lk(g_tune_mtx);
+			g_tune[key] = { chunk, tuned };
+		}
+	}
+	p->chunk = chunk;
+	p->tuned_ms = tuned;
+	p->launches = count_launches(ngrids, grids, pt_offsets, chunk);
+	cudaError_t e = cudaMalloc(&p->counters, sizeof(unsigned long long) * std::max(p->launches, 1));
+	if (e != cudaSuccess) { free_plan(p); return fail(SGI_E_NOMEM, "cudaMalloc failed: %s", cudaGetErrorString(e)); }
+	cudaStream_t cs = nullptr;
+	e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+	if (e != cudaSuccess) { free_plan(p); return fail(SGI_E_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e)); }
+	e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+	if (e == cudaSuccess)
+	{
+		int n = 0;
+		rc = launch_forward(ngrids, grids, pt_offsets, x, out, precision, cs, chunk, p->counters, &n);
+		cudaGraph_t g = nullptr;
+		e = cudaStreamEndCapture(cs, &g);
+		p->graph = g;
+		if (!rc && e == cudaSuccess && n != p->launches) rc = fail(SGI_E_CUDA, "plan recorded %d launches, expected %d", n, p->launches);
+	}
+	cudaStreamDestroy(cs);
+	if (rc) { free_plan(p); return rc; }
+	if (e != cudaSuccess) { free_plan(p); return fail(SGI_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e)); }
+	e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+	if (e != cudaSuccess) { free_plan(p); return fail(SGI_E_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(e)); }
+	*out_plan = p;
+	return SGI_OK;
+}
+
+extern "C" int sgi_plan_launch(sgi_plan_t p, void* stream)
+{
+	clear_error();
+	if (!p) return fail(SGI_E_INVALID, "null plan");
+	DeviceGuard guard(p->device);
+	CUDA_TRY(cudaGraphLaunch(p->exec, (cudaStream_t)stream));
+	g_stats = sgi_launch_stats{};
+	g_stats.kernels = p->launches;
+	return SGI_OK;
+}
+
+extern "C" int sgi_plan_info(sgi_plan_t p, int* chunk_rows_out, int* launches, float* tuned_ms)
+{
+	clear_error();
+	if (!p) return fail(SGI_E_INVALID, "null plan");
+	if (chunk_rows_out) *chunk_rows_out = p->chunk;
+	if (launches) *launches = p->launches;
+	if (tuned_ms) *tuned_ms = p->tuned_ms;
+	return SGI_OK;
+}
+
+extern "C" void sgi_plan_destroy(sgi_plan_t p)
+{
+	if (!p) return;
+	DeviceGuard guard(p->device);
+	free_plan(p);
 }

@@ -74,6 +74,10 @@ def _load():
         "sgi_active_count": (I, [P, LL, P, P, P]),
         "sgi_last_launch": (I, [ctypes.POINTER(LaunchStats)]),
         "sgi_set_chunk_rows": (I, [I]),
+        "sgi_plan_create": (I, [I, P, P, P, P, I, I, P, ctypes.POINTER(P)]),
+        "sgi_plan_launch": (I, [P, P]),
+        "sgi_plan_info": (I, [P, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_float)]),
+        "sgi_plan_destroy": (None, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -305,6 +309,38 @@ def backward(grid, x, gout, want_x=True, want_surplus=True, stream=None):
                             gx.data_ptr() if gx is not None else None,
                             gs.data_ptr() if gs is not None else None, _stream_ptr(stream)))
     return gx, gs
+
+
+class Plan:
+    """A forward call recorded into a CUDA graph (see sgi_plan_create); x and out
+    are fixed at creation, every launch() recomputes out from x."""
+
+    def __init__(self, grids, x, out, counts=None, precision=FP64, chunk_rows=-1, stream=None):
+        if not isinstance(grids, (list, tuple)):
+            grids = [grids]
+        if counts is None:
+            counts = [x.shape[0]]
+        self.offs = np.zeros(len(grids) + 1, np.int64)
+        self.offs[1:] = np.cumsum(counts)
+        self.grids, self.x, self.out = list(grids), x, out   # keep buffers alive
+        self._arr = _grid_array(grids)
+        h = ctypes.c_void_p()
+        _check(lib.sgi_plan_create(len(grids), self._arr, self.offs.ctypes.data, x.data_ptr(), out.data_ptr(),
+                                   precision, chunk_rows, _stream_ptr(stream), ctypes.byref(h)))
+        self._h = h
+        c, n, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        _check(lib.sgi_plan_info(h, ctypes.byref(c), ctypes.byref(n), ctypes.byref(t)))
+        self.chunk_rows, self.launches, self.tuned_ms = c.value, n.value, t.value
+
+    def launch(self, stream=None):
+        _check(lib.sgi_plan_launch(self._h, _stream_ptr(stream)))
+        return self.out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.sgi_plan_destroy(h)
+            self._h = None
 
 
 def set_chunk_rows(rows):

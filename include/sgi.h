@@ -207,6 +207,27 @@ int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* o
  * setting.  No reference counterpart. */
 int sgi_set_chunk_rows(int rows);
 
+/* Plans: one forward call recorded into a CUDA graph and replayed.
+ * sgi_plan_create records every launch of sgi_interpolate(ngrids, grids,
+ * pt_offsets, x, out, precision) (work-counter clears and node-chunk launches,
+ * with work counters owned by the plan) into a graph; sgi_plan_launch replays
+ * it on `stream` with one cudaGraphLaunch.  x and out are baked into the
+ * graph: later replays read the same x buffer and write the same out buffer.
+ * chunk_rows >= 0 fixes the node-chunk size (0 = none); chunk_rows < 0 lets the
+ * autotuner choose it: the first time a (dim, largest nno, TotalDof,
+ * precision, point count) key is seen, candidate chunk sizes (none, and rows
+ * filling 1/4, 1/2, 1 and 2 L2s) are timed on the given inputs (which runs the
+ * forward, overwriting out) and the fastest is cached for the process.
+ * Replays of one plan must not overlap each other.  No reference counterpart
+ * (the reference relaunched per call and JIT-compiled per dimension,
+ * LinearBasis/cuda/src/JIT.cpp:223-257). */
+typedef struct sgi_plan* sgi_plan_t;
+int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, int precision, int chunk_rows, void* stream, sgi_plan_t* plan);
+int sgi_plan_launch(sgi_plan_t plan, void* stream);
+int sgi_plan_info(sgi_plan_t plan, int* chunk_rows, int* launches, float* tuned_ms);
+void sgi_plan_destroy(sgi_plan_t plan);
+
 /* Launch statistics of this thread's last sgi_interpolate/sgi_backward call. */
 typedef struct sgi_launch_stats
 {

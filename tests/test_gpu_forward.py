@@ -204,3 +204,39 @@ def test_chunked_walk_bit_exact(cuda, rows):
         ref = O.Gold(*h.arrays()).interpolate(X[sl])
         assert np.array_equal(out[sl], ref), k
         assert O.rel_error(out32[sl], ref)[0] <= FP32C_TOL, k
+
+
+@pytest.mark.parametrize("chunk_rows", [-1, 0, 777])
+def test_graph_plan_bit_exact_and_replayable(cuda, chunk_rows):
+    """A forward call recorded into a CUDA graph (autotuned or fixed chunks)
+    replays to the bits of the direct call with the same node chunks; the FP64
+    form also to gold's bits, whatever the chunks."""
+    import torch
+    hosts = [H.HostGrid.adaptive(59, 9000, 128, seed=50), H.HostGrid.adaptive(59, 4000, 128, seed=51)]
+    grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
+    counts = [4000, 1000]
+    X = H.gen_points(59, 5000, kind=2, seed=52)
+    x = torch.from_numpy(X).cuda()
+    for precision in (H.FP64, H.FP32C):
+        out = torch.full((5000, 128), float("nan"), dtype=torch.float64, device="cuda")
+        plan = H.Plan(grids, x, out, counts=counts, precision=precision, chunk_rows=chunk_rows)
+        if chunk_rows >= 0:
+            assert plan.chunk_rows == chunk_rows
+        prev = H.set_chunk_rows(plan.chunk_rows)
+        try:
+            direct = H.interpolate(grids, x, counts=counts, precision=precision).cpu().numpy()
+        finally:
+            H.set_chunk_rows(prev)
+        for _ in range(3):
+            out.fill_(float("nan"))
+            plan.launch()
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            assert np.array_equal(got, direct), precision
+        for k, (h, sl) in enumerate(zip(hosts, (slice(0, 4000), slice(4000, 5000)))):
+            sub = np.arange(sl.start, sl.stop)[::37]
+            ref = O.Gold(*h.arrays()).interpolate(X[sub])
+            if precision == H.FP64:
+                assert np.array_equal(got[sub], ref), k
+            else:
+                assert O.rel_error(got[sub], ref)[0] <= FP32C_TOL, k
