@@ -270,7 +270,8 @@ def run_gpu(args):
             "clocks": clocks,
             "setup_s": {"generate": round(t_gen, 2), "layout_and_upload": round(t_upload, 2),
                         "autotune_and_capture": round(t_tune, 2)},
-            "plans": {"fp32c": {"chunk_rows": plan32.chunk_rows, "launches": plan32.launches},
+            "plans": {"fp32c": {"chunk_rows": plan32.chunk_rows, "variant": plan32.variant,
+                                "launches": plan32.launches},
                       "fp64": {"chunk_rows": plan64.chunk_rows, "launches": plan64.launches},
                       "note": "each step replays one CUDA graph holding all node-chunk launches"},
         }

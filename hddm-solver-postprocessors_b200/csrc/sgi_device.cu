@@ -92,32 +92,69 @@ __device__ __forceinline__ int find_grid(const FwdArgs& a, long long p)
 // A node whose tree parent lies before `a` ("chunk root") is checked on all its
 // components, since its ancestors are not walked; inside the range a node is
 // reached only when all its ancestors in the range are active.
+// Product of a hit node's hats in dimension order (the gold loop's `temp`).
+// Components are fetched four at a time, so a node costs one memory round
+// trip per four components instead of one per component.
+__device__ __forceinline__ double node_weight(const GridDesc& G, const double* xs, uint32_t cptr, uint32_t ncomp)
+{
+	double w = 1.0;
+	for (uint32_t c0 = 0; c0 < ncomp; c0 += 4)
+	{
+		uint2 cp[4];
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			cp[q] = c0 + q < ncomp ? __ldg(G.comps + cptr + c0 + q) : make_uint2(0u, 0u);
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			if (c0 + q < ncomp) w = __dmul_rn(w, hat(xs[cp[q].x], cp[q].y));
+	}
+	return w;
+}
+
+// True when every hat of the node is positive at x (a product test would
+// accept an even number of negative hats).
+__device__ __forceinline__ bool node_active(const GridDesc& G, const double* xs, uint32_t cptr, uint32_t ncomp)
+{
+	bool act = true;
+	for (uint32_t c0 = 0; c0 < ncomp && act; c0 += 4)
+	{
+		uint2 cp[4];
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			cp[q] = c0 + q < ncomp ? __ldg(G.comps + cptr + c0 + q) : make_uint2(0u, 0u);
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			if (c0 + q < ncomp) act = act && hat(xs[cp[q].x], cp[q].y) > 0.0;
+	}
+	return act;
+}
+
 template <class OnHits>
 __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, int a, int b,
 	OnHits&& on_hits)
 {
 	int n0 = a;
+	// the next window's records are fetched before this window's hits are
+	// accumulated, so that their latency overlaps the row gathers
+	uint4 rn = make_uint4(0u, 0u, 0u, 0u);
+	int pn = -1;
+	if (n0 + lane < b)
+	{
+		rn = __ldg(G.rec + n0 + lane);
+		if (a > 0) pn = __ldg(G.parent + n0 + lane);
+	}
 	while (n0 < b)
 	{
 		const int idx = n0 + lane;
 		const bool valid = idx < b;
-		uint4 r = make_uint4(0u, 0u, 0u, 0u);
-		if (valid) r = __ldg(G.rec + idx);
+		const uint4 r = rn;
 		const uint32_t ncomp = r.z & 0xffu;
-		const bool chunk_root = a > 0 && valid && __ldg(G.parent + idx) < a;
+		const bool chunk_root = a > 0 && valid && pn < a;
 		bool act = false;
 		if (valid)
 		{
 			if (r.z & NODE_DEAD) act = false;
-			else if ((r.z & NODE_MULTI) || chunk_root)
-			{
-				act = true;
-				for (uint32_t c = 0; c < ncomp && act; c++)
-				{
-					const uint2 cp = __ldg(G.comps + r.y + c);
-					act = hat(xs[cp.x], cp.y) > 0.0;
-				}
-			}
+			else if ((r.z & NODE_MULTI) || chunk_root) act = node_active(G, xs, r.y, ncomp);
 			else if (r.z & NODE_ALWAYS) act = true;
 			else act = hat(xs[r.z >> 16], r.w) > 0.0;
 		}
@@ -133,19 +170,18 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 		if (lane == 0) exc = 0u;
 		const bool hit = act && exc <= (unsigned)idx;
 		const unsigned mask = __ballot_sync(FULL, hit);
-		double w = 0.0;
-		if (hit)
-		{
-			w = 1.0;
-			for (uint32_t c = 0; c < ncomp; c++)
-			{
-				const uint2 cp = __ldg(G.comps + r.y + c);
-				w = __dmul_rn(w, hat(xs[cp.x], cp.y));
-			}
-		}
-		if (mask) on_hits(mask, n0, w, r);
 		const unsigned last = __shfl_sync(FULL, inc, 31);
-		n0 = max(n0 + 32, (int)last);
+		const int nnext = max(n0 + 32, (int)last);
+		rn = make_uint4(0u, 0u, 0u, 0u);
+		pn = -1;
+		if (nnext + lane < b)
+		{
+			rn = __ldg(G.rec + nnext + lane);
+			if (a > 0) pn = __ldg(G.parent + nnext + lane);
+		}
+		const double w = hit ? node_weight(G, xs, r.y, ncomp) : 0.0;
+		if (mask) on_hits(mask, n0, w, r);
+		n0 = nnext;
 	}
 }
 
@@ -294,8 +330,8 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 // pair's four FP32 products are summed in FP32 (the split keeps the weight's
 // rounding out of the result), and the pair sum is added to the output's FP64
 // running sum, which also carries the sums across node chunks.
-template <int V, int E>
-__global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__ FwdArgs a)
+template <int V, int E, int Q, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_constant__ FwdArgs a)
 {
 	extern __shared__ double smem[];
 	const int lane = threadIdx.x & 31;
@@ -349,39 +385,46 @@ __global__ void __launch_bounds__(BLOCK) fwd_f32c_kernel(const __grid_constant__
 #pragma unroll
 						for (int e = 0; e < E; e++) acc[v][e] = fma(wk, sv[v][e], acc[v][e]);
 				}
+				// Q rows in flight; each pair of hits is summed in FP32 and
+				// added to the FP64 running sum
 				while (fm)
 				{
-					const int k0 = __ffs(fm) - 1;
-					fm &= fm - 1;
-					const bool two = fm != 0u;
-					const int k1 = two ? __ffs(fm) - 1 : k0;
-					if (two) fm &= fm - 1;
-					const double w0 = __shfl_sync(FULL, w, k0);
-					const double w1 = two ? __shfl_sync(FULL, w, k1) : 0.0;
-					const float w0h = __double2float_rn(w0), w0l = __double2float_rn(w0 - (double)w0h);
-					const float w1h = __double2float_rn(w1), w1l = __double2float_rn(w1 - (double)w1h);
-					const float* row0 = G.s32 + (size_t)(n0 + k0) * G.ld + a.o_begin;
-					const float* row1 = G.s32 + (size_t)(n0 + k1) * G.ld + a.o_begin;
-					float s0[V][E], s1[V][E];
+					int k[Q];
+					float wh[Q], wl[Q];
+					const float* row[Q];
+#pragma unroll
+					for (int q = 0; q < Q; q++)
+					{
+						const bool have = fm != 0u;
+						k[q] = have ? __ffs(fm) - 1 : 0;
+						if (have) fm &= fm - 1;
+						const double wq = have ? __shfl_sync(FULL, w, k[q]) : 0.0;
+						wh[q] = __double2float_rn(wq);
+						wl[q] = __double2float_rn(wq - (double)wh[q]);
+						row[q] = G.s32 + (size_t)(n0 + k[q]) * G.ld + a.o_begin;
+					}
+					float sv[Q][V][E];
 #pragma unroll
 					for (int v = 0; v < V; v++)
 					{
 						const int o = out_col<E>(v, lane);
 						const bool in = a.o_begin + o < G.ld;
-						load_row<E>(row0, o, in, s0[v]);
-						load_row<E>(row1, o, in, s1[v]);
+#pragma unroll
+						for (int q = 0; q < Q; q++) load_row<E>(row[q], o, in, sv[q][v]);
 					}
 #pragma unroll
 					for (int v = 0; v < V; v++)
 #pragma unroll
 						for (int e = 0; e < E; e++)
-						{
-							float f = __fmul_rn(w0l, s0[v][e]);
-							f = __fmaf_rn(w1l, s1[v][e], f);
-							f = __fmaf_rn(w1h, s1[v][e], f);
-							f = __fmaf_rn(w0h, s0[v][e], f);
-							acc[v][e] = __dadd_rn(acc[v][e], (double)f);
-						}
+#pragma unroll
+							for (int q = 0; q < Q; q += 2)
+							{
+								float f = __fmul_rn(wl[q], sv[q][v][e]);
+								f = __fmaf_rn(wl[q + 1], sv[q + 1][v][e], f);
+								f = __fmaf_rn(wh[q + 1], sv[q + 1][v][e], f);
+								f = __fmaf_rn(wh[q], sv[q][v][e], f);
+								acc[v][e] = __dadd_rn(acc[v][e], (double)f);
+							}
 				}
 			});
 		}
@@ -618,16 +661,25 @@ std::atomic<int> g_chunk_override{[]() { const char* e = getenv("SGI_CHUNK_ROWS"
 
 int chunk_rows_env() { return g_chunk_override.load(); }
 
-// Forward kernel for a pass of `cols` outputs with row stride ld.
-void (*select_fwd(int precision, int ld, int cols))(FwdArgs)
+// Forward kernel for a pass of `cols` outputs with row stride ld.  variant
+// (FP32C only) trades fine rows in flight per warp against warps per SM:
+// 0 = two rows, registers as needed; 1 = four rows, at least 3 blocks per SM;
+// 2 = two rows, at least 4 blocks per SM.  Plans time all three.
+constexpr int NVARIANTS = 3;
+template <int V, int E>
+void (*f32c_variant(int variant))(FwdArgs)
 {
-	if (ld <= 32)
-		return precision == SGI_FP64 ? fwd_f64_kernel<1, 1> : fwd_f32c_kernel<1, 1>;
-	if (cols <= 64)
-		return precision == SGI_FP64 ? fwd_f64_kernel<1, 2> : fwd_f32c_kernel<1, 2>;
-	if (cols <= 128)
-		return precision == SGI_FP64 ? fwd_f64_kernel<2, 2> : fwd_f32c_kernel<2, 2>;
-	return precision == SGI_FP64 ? fwd_f64_kernel<4, 2> : fwd_f32c_kernel<4, 2>;
+	return variant == 1 ? fwd_f32c_kernel<V, E, 4, 3> : variant == 2 ? fwd_f32c_kernel<V, E, 2, 4>
+	                                                                 : fwd_f32c_kernel<V, E, 2, 1>;
+}
+
+void (*select_fwd(int precision, int ld, int cols, int variant = 0))(FwdArgs)
+{
+	const bool f64 = precision == SGI_FP64;
+	if (ld <= 32) return f64 ? fwd_f64_kernel<1, 1> : f32c_variant<1, 1>(variant);
+	if (cols <= 64) return f64 ? fwd_f64_kernel<1, 2> : f32c_variant<1, 2>(variant);
+	if (cols <= 128) return f64 ? fwd_f64_kernel<2, 2> : f32c_variant<2, 2>(variant);
+	return f64 ? fwd_f64_kernel<4, 2> : f32c_variant<4, 2>(variant);
 }
 
 int pick_R(int cols)
@@ -832,7 +884,7 @@ int check_set(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets)
 // from the device workspace's ring.
 int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets, const double* x,
 	double* out, int precision, cudaStream_t stream, int chunk = -1, unsigned long long* counters = nullptr,
-	int* nlaunch = nullptr)
+	int* nlaunch = nullptr, int variant = 2)
 {
 	const sgi_grid* g0 = grids[0];
 	DeviceWork* W = nullptr;
@@ -869,7 +921,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 			a.chunk_len = clen;
 			a.counter = counters ? counters + launches : W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS));
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, W->sms, &blocks);
@@ -1190,6 +1242,7 @@ struct sgi_plan
 {
 	int device = 0;
 	int chunk = 0;
+	int variant = 0;
 	int launches = 0;
 	unsigned long long* counters = nullptr;
 	cudaGraph_t graph = nullptr;
@@ -1209,16 +1262,17 @@ struct TuneKey
 	}
 };
 std::mutex g_tune_mtx;
-std::map<TuneKey, std::pair<int, float>> g_tune;
+struct TuneResult { int chunk, variant; float ms; };
+std::map<TuneKey, TuneResult> g_tune;
 
 int time_forward(int ngrids, const sgi_grid_t* grids, const long long* offs, const double* x, double* out,
-	int precision, cudaStream_t s, int chunk, float* ms)
+	int precision, cudaStream_t s, int chunk, int variant, float* ms)
 {
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	CUDA_TRY(cudaEventCreate(&e0));
 	CUDA_TRY(cudaEventCreate(&e1));
-	int rc = launch_forward(ngrids, grids, offs, x, out, precision, s, chunk);
-	if (!rc) { cudaEventRecord(e0, s); rc = launch_forward(ngrids, grids, offs, x, out, precision, s, chunk); }
+	int rc = launch_forward(ngrids, grids, offs, x, out, precision, s, chunk, nullptr, nullptr, variant);
+	if (!rc) { cudaEventRecord(e0, s); rc = launch_forward(ngrids, grids, offs, x, out, precision, s, chunk, nullptr, nullptr, variant); }
 	if (!rc) { cudaEventRecord(e1, s); cudaEventSynchronize(e1); cudaEventElapsedTime(ms, e0, e1); }
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
@@ -1257,41 +1311,57 @@ extern "C" int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long l
 	sgi_plan* p = new sgi_plan;
 	p->device = grids[0]->device;
 	float tuned = 0.f;
-	int chunk = chunk_rows_req;
-	if (chunk < 0)
+	int chunk = chunk_rows_req, variant = 0;
 	{
 		const TuneKey key{ grids[0]->dim, maxnno, grids[0]->TD, precision, npts };
 		bool hit = false;
+		if (chunk < 0)
 		{
 			std::lock_guard<std::mutex> lk(g_tune_mtx);
 			auto it = g_tune.find(key);
-			if (it != g_tune.end()) { chunk = it->second.first; tuned = it->second.second; hit = true; }
+			if (it != g_tune.end()) { chunk = it->second.chunk; variant = it->second.variant; tuned = it->second.ms; hit = true; }
 		}
 		if (!hit)
 		{
-			// candidates: no chunks, and chunks whose rows fill 1/4 .. 2 x the L2
-			const long long row = (long long)grids[0]->ld * (precision == SGI_FP64 ? 8 : 4);
-			std::vector<int> cand{ 0 };
-			for (double f : { 0.25, 0.5, 1.0, 2.0 })
+			// candidates: no chunks, and chunks whose rows fill 1/4 .. 2 x the
+			// L2 (or the requested chunk); kernel variants for FP32C
+			std::vector<int> cand;
+			if (chunk >= 0) cand.push_back(chunk);
+			else
 			{
-				const long long r = std::max(1024ll, (long long)(W->l2_bytes * f / row));
-				if (r < maxnno) cand.push_back((int)r);
+				const long long row = (long long)grids[0]->ld * (precision == SGI_FP64 ? 8 : 4);
+				cand.push_back(0);
+				for (double f : { 0.25, 0.5, 1.0, 2.0 })
+				{
+					const long long r = std::max(1024ll, (long long)(W->l2_bytes * f / row));
+					if (r < maxnno) cand.push_back((int)r);
+				}
 			}
-			float best = 0.f;
-			int best_c = 0;
-			for (size_t q = 0; q < cand.size(); q++)
+			const int nvar = precision == SGI_FP32C ? NVARIANTS : 1;
+			chunk = cand[0];
+			variant = 0;
+			if (cand.size() * nvar > 1)
 			{
-				float ms = 0.f;
-				rc = time_forward(ngrids, grids, pt_offsets, x, out, precision, stream, cand[q], &ms);
-				if (rc) { free_plan(p); return rc; }
-				if (q == 0 || ms < best) { best = ms; best_c = cand[q]; }
+				float best = 0.f;
+				bool first = true;
+				for (int c : cand)
+					for (int v = 0; v < nvar; v++)
+					{
+						float ms = 0.f;
+						rc = time_forward(ngrids, grids, pt_offsets, x, out, precision, stream, c, v, &ms);
+						if (rc) { free_plan(p); return rc; }
+						if (first || ms < best) { best = ms; chunk = c; variant = v; first = false; }
+					}
+				tuned = best;
+				if (chunk_rows_req < 0)
+				{
+					std::lock_guard<std::mutex> lk(g_tune_mtx);
+					g_tune[key] = TuneResult{ chunk, variant, tuned };
+				}
 			}
-			chunk = best_c;
-			tuned = best;
-			std::lock_guard<std::mutex> lk(g_tune_mtx);
-			g_tune[key] = { chunk, tuned };
 		}
 	}
+	p->variant = variant;
 	p->chunk = chunk;
 	p->tuned_ms = tuned;
 	p->launches = count_launches(ngrids, grids, pt_offsets, chunk);
@@ -1304,7 +1374,7 @@ extern "C" int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long l
 	if (e == cudaSuccess)
 	{
 		int n = 0;
-		rc = launch_forward(ngrids, grids, pt_offsets, x, out, precision, cs, chunk, p->counters, &n);
+		rc = launch_forward(ngrids, grids, pt_offsets, x, out, precision, cs, chunk, p->counters, &n, variant);
 		cudaGraph_t g = nullptr;
 		e = cudaStreamEndCapture(cs, &g);
 		p->graph = g;
@@ -1330,10 +1400,11 @@ extern "C" int sgi_plan_launch(sgi_plan_t p, void* stream)
 	return SGI_OK;
 }
 
-extern "C" int sgi_plan_info(sgi_plan_t p, int* chunk_rows_out, int* launches, float* tuned_ms)
+extern "C" int sgi_plan_info(sgi_plan_t p, int* chunk_rows_out, int* variant, int* launches, float* tuned_ms)
 {
 	clear_error();
 	if (!p) return fail(SGI_E_INVALID, "null plan");
+	if (variant) *variant = p->variant;
 	if (chunk_rows_out) *chunk_rows_out = p->chunk;
 	if (launches) *launches = p->launches;
 	if (tuned_ms) *tuned_ms = p->tuned_ms;

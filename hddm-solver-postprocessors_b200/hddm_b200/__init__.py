@@ -76,7 +76,7 @@ def _load():
         "sgi_set_chunk_rows": (I, [I]),
         "sgi_plan_create": (I, [I, P, P, P, P, I, I, P, ctypes.POINTER(P)]),
         "sgi_plan_launch": (I, [P, P]),
-        "sgi_plan_info": (I, [P, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_float)]),
+        "sgi_plan_info": (I, [P, _c_int_p, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_float)]),
         "sgi_plan_destroy": (None, [P]),
     }
     for name, (res, args) in sig.items():
@@ -328,9 +328,9 @@ class Plan:
         _check(lib.sgi_plan_create(len(grids), self._arr, self.offs.ctypes.data, x.data_ptr(), out.data_ptr(),
                                    precision, chunk_rows, _stream_ptr(stream), ctypes.byref(h)))
         self._h = h
-        c, n, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
-        _check(lib.sgi_plan_info(h, ctypes.byref(c), ctypes.byref(n), ctypes.byref(t)))
-        self.chunk_rows, self.launches, self.tuned_ms = c.value, n.value, t.value
+        c, v, n, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        _check(lib.sgi_plan_info(h, ctypes.byref(c), ctypes.byref(v), ctypes.byref(n), ctypes.byref(t)))
+        self.chunk_rows, self.variant, self.launches, self.tuned_ms = c.value, v.value, n.value, t.value
 
     def launch(self, stream=None):
         _check(lib.sgi_plan_launch(self._h, _stream_ptr(stream)))

@@ -216,8 +216,9 @@ int sgi_set_chunk_rows(int rows);
  * chunk_rows >= 0 fixes the node-chunk size (0 = none); chunk_rows < 0 lets the
  * autotuner choose it: the first time a (dim, largest nno, TotalDof,
  * precision, point count) key is seen, candidate chunk sizes (none, and rows
- * filling 1/4, 1/2, 1 and 2 L2s) are timed on the given inputs (which runs the
- * forward, overwriting out) and the fastest is cached for the process.
+ * filling 1/4, 1/2, 1 and 2 L2s), and for FP32C the kernel variants, are timed
+ * on the given inputs (which runs the forward, overwriting out) and the
+ * fastest is cached for the process.
  * Replays of one plan must not overlap each other.  No reference counterpart
  * (the reference relaunched per call and JIT-compiled per dimension,
  * LinearBasis/cuda/src/JIT.cpp:223-257). */
@@ -225,7 +226,10 @@ typedef struct sgi_plan* sgi_plan_t;
 int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
 	const double* x, double* out, int precision, int chunk_rows, void* stream, sgi_plan_t* plan);
 int sgi_plan_launch(sgi_plan_t plan, void* stream);
-int sgi_plan_info(sgi_plan_t plan, int* chunk_rows, int* launches, float* tuned_ms);
+/* The plan's node-chunk size, kernel variant (FP32C: 0 = two fine rows in
+ * flight per warp, 1 = four rows at >= 3 blocks per SM, 2 = two rows at >= 4
+ * blocks per SM), launches per replay and the tuned time of one call (ms). */
+int sgi_plan_info(sgi_plan_t plan, int* chunk_rows, int* variant, int* launches, float* tuned_ms);
 void sgi_plan_destroy(sgi_plan_t plan);
 
 /* Launch statistics of this thread's last sgi_interpolate/sgi_backward call. */
