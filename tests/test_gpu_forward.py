@@ -240,3 +240,22 @@ def test_graph_plan_bit_exact_and_replayable(cuda, chunk_rows):
                 assert np.array_equal(got[sub], ref), k
             else:
                 assert O.rel_error(got[sub], ref)[0] <= FP32C_TOL, k
+
+
+def test_wide_component_form_bit_exact(cuda):
+    """Grids whose hat scales are not powers of two (or exceed the 32-bit
+    packed form) use the wide components; still gold-exact."""
+    rng = np.random.default_rng(8)
+    dim = 6
+    idx = np.zeros((300, 2 * dim), np.int32)
+    for n in range(1, 300):
+        for k in rng.choice(dim, rng.integers(1, 4), replace=False):
+            idx[n, k] = int(rng.integers(1, 9))          # i = 3, 5, 6, ... too
+            idx[n, dim + k] = int(rng.integers(0, idx[n, k] + 1))
+    sur = rng.uniform(-1, 1, (300, 16))
+    hg = H.HostGrid.from_dense(idx, sur)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    X = rng.random((400, dim))
+    ref = O.Gold(idx, sur).interpolate(X)
+    assert np.array_equal(_run(g, X), ref)
+    assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
