@@ -348,12 +348,132 @@ def run_reference(args):
     }))
 
 
+def _plan_time(H, torch, plan, stream, steps, warmup):
+    for _ in range(warmup):
+        plan.launch(stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        plan.launch(stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _rel_err(torch, a, b):
+    den = torch.maximum(b.abs(), 1e-3 * b.abs().amax(dim=1, keepdim=True))
+    e = ((a - b).abs() / den).amax(dim=1)
+    return float(e.max()), float(e.pow(2).mean().sqrt())
+
+
+def run_c2(args):
+    """8 multistate grids (d=30, nno log-uniform in [20k, 200k], TotalDof=64), ragged
+    batches of 1..100k uniform points per grid, one persistent launch per call."""
+    import torch
+    import hddm_b200 as H
+    dev = torch.device("cuda", 0)
+    rng = np.random.Generator(np.random.PCG64(2))
+    nnos = np.exp(rng.uniform(np.log(20_000), np.log(200_000), 8)).astype(int)
+    counts = rng.integers(1, 100_001, 8)
+    hosts = [H.HostGrid.adaptive(30, int(n), 64, seed=200 + k) for k, n in enumerate(nnos)]
+    grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
+    X = H.gen_points(30, int(counts.sum()), kind=0, seed=2)
+    x = torch.from_numpy(X).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    o32 = torch.empty((x.shape[0], 64), dtype=torch.float64, device=dev)
+    o64 = torch.empty_like(o32)
+    p32 = H.Plan(grids, x, o32, counts=list(counts), precision=H.FP32C, stream=stream)
+    p64 = H.Plan(grids, x, o64, counts=list(counts), precision=H.FP64, stream=stream)
+    ms32 = _plan_time(H, torch, p32, stream, args.steps, args.warmup)
+    ms64 = _plan_time(H, torch, p64, stream, args.steps, args.warmup)
+    emax, erms = _rel_err(torch, o32, o64)
+    npts = int(counts.sum())
+    print(json.dumps({"workload": "C2: 8 multistate grids d=30, TotalDof=64, ragged batches", "grids_nno": nnos.tolist(),
+                      "points_per_grid": counts.tolist(), "points": npts,
+                      "fp32c": {"ms": ms32, "points_per_s": npts / ms32 * 1e3, "variant": p32.variant,
+                                "chunk_rows": p32.chunk_rows, "launches": p32.launches},
+                      "fp64": {"ms": ms64, "points_per_s": npts / ms64 * 1e3, "launches": p64.launches},
+                      "fp32c_vs_gold_exact_fp64": {"max_rel_err": emax, "rms_rel_err": erms}}))
+
+
+def run_c3(args):
+    """Backward: d=59 adaptive grid of 300k nodes, TotalDof=128, 32768 points kept 1e-6
+    from every kink; dL/dx and dL/dsurplus of L = sum c * f with c ~ N(0,1)."""
+    import torch
+    import hddm_b200 as H
+    dev = torch.device("cuda", 0)
+    hg = H.HostGrid.adaptive(59, 300_000, 128, seed=3)
+    g = H.Grid(hg)
+    X = H.gen_points(59, 32768, kind=0, seed=3, kink_reject=1e-6)
+    C = np.random.Generator(np.random.PCG64(3)).standard_normal((32768, 128))
+    x = torch.from_numpy(X).to(dev)
+    c = torch.from_numpy(C).to(dev)
+    for _ in range(args.warmup):
+        H.backward(g, x, c)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        gx, gs = H.backward(g, x, c)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    e0.record()
+    for _ in range(args.steps):
+        H.interpolate(g, x)
+    e1.record()
+    torch.cuda.synchronize()
+    fms = e0.elapsed_time(e1) / args.steps
+    pairs = float(H.active_count(g, x).double().sum())
+    print(json.dumps({"workload": "C3: backward, d=59, 300k nodes, TotalDof=128, 32768 points",
+                      "backward_ms": ms, "forward_fp64_ms": fms, "active_pairs": pairs,
+                      "backward_points_per_s": 32768 / ms * 1e3,
+                      "grad_norms": {"dx": float(gx.norm()), "dsurplus": float(gs.norm())}}))
+
+
+def run_multistate(args):
+    """The reference's own call shape: one point per state across 16 states
+    (d=59, TotalDof=118, 200k nodes each), per-call latency."""
+    import ctypes
+    import torch
+    import hddm_b200 as H
+    dev = torch.device("cuda", 0)
+    ns = 16
+    hosts = [H.HostGrid.adaptive(59, 200_000, 118, seed=300 + k) for k in range(ns)]
+    grids = [H.Grid(h) for h in hosts]
+    X = H.gen_points(59, ns, kind=0, seed=5)
+    arr = (ctypes.c_void_p * ns)(*[g.handle.value for g in grids])
+    offs = np.arange(ns + 1, dtype=np.int64)
+    xh = np.ascontiguousarray(X)
+    outh = np.zeros((ns, 118))
+    for _ in range(args.warmup):
+        H.lib.sgi_interpolate_host(ns, arr, offs.ctypes.data, xh.ctypes.data, outh.ctypes.data, H.FP64)
+    reps = max(args.steps, 50)
+    t = time.perf_counter()
+    for _ in range(reps):
+        rc = H.lib.sgi_interpolate_host(ns, arr, offs.ctypes.data, xh.ctypes.data, outh.ctypes.data, H.FP64)
+    host_s = (time.perf_counter() - t) / reps
+    x = torch.from_numpy(X).to(dev)
+    out = torch.empty((ns, 118), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    plan = H.Plan(grids, x, out, counts=[1] * ns, precision=H.FP64, chunk_rows=0, stream=stream)
+    dev_ms = _plan_time(H, torch, plan, stream, reps, args.warmup)
+    print(json.dumps({"workload": "multistate call: 16 states x 1 point, d=59, TotalDof=118, 200k nodes per state",
+                      "rc": rc, "host_call_s": host_s, "host_s_per_state": host_s / ns,
+                      "graph_replay_ms": dev_ms, "graph_s_per_state": dev_ms * 1e-3 / ns,
+                      "reference_published_s_per_state": {"large, cuda (daint)": 2.754e-4,
+                                                          "large, avx2 (daint)": 4.234e-3}}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate"],
+                    help="c4 (default) is the benchmark line; the others print their own measurements")
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -366,6 +486,12 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c2":
+        run_c2(args)
+    elif args.workload == "c3":
+        run_c3(args)
+    elif args.workload == "multistate":
+        run_multistate(args)
     else:
         run_gpu(args)
 

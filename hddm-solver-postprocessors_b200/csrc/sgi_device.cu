@@ -55,6 +55,8 @@ struct GridDesc
 	const double* s64c;          // FP64 copies of the coarse rows (FP32C form)
 	const uint32_t* coarse_index; // row of node n in s64c, for coarse nodes
 	const int* parent;           // tree parent per node (-1 for roots)
+	const float* rowmax;         // largest |surplus| of each row (FP32C), or null
+	float skip_below;            // FP32C drops fine terms with |w| * rowmax below this
 	long long pt_begin;
 	int nno;
 	int ld;
@@ -138,16 +140,19 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 	// accumulated, so that their latency overlaps the row gathers
 	uint4 rn = make_uint4(0u, 0u, 0u, 0u);
 	int pn = -1;
+	float mn = 0.f;
 	if (n0 + lane < b)
 	{
 		rn = __ldg(G.rec + n0 + lane);
 		if (a > 0) pn = __ldg(G.parent + n0 + lane);
+		if (G.rowmax) mn = __ldg(G.rowmax + n0 + lane);
 	}
 	while (n0 < b)
 	{
 		const int idx = n0 + lane;
 		const bool valid = idx < b;
 		const uint4 r = rn;
+		const float rm = mn;
 		const uint32_t ncomp = r.z & 0xffu;
 		const bool chunk_root = a > 0 && valid && pn < a;
 		bool act = false;
@@ -178,9 +183,10 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 		{
 			rn = __ldg(G.rec + nnext + lane);
 			if (a > 0) pn = __ldg(G.parent + nnext + lane);
+			if (G.rowmax) mn = __ldg(G.rowmax + nnext + lane);
 		}
 		const double w = hit ? node_weight(G, xs, r.y, ncomp) : 0.0;
-		if (mask) on_hits(mask, n0, w, r);
+		if (mask) on_hits(mask, n0, w, r, rm);
 		n0 = nnext;
 	}
 }
@@ -275,7 +281,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 		if (!ok && !first) continue;        // NaN already written by the first chunk
 		if (ok)
 		{
-			traverse(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&)
+			traverse(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&, float)
 			{
 				// two hits per step, both rows loaded before either is added, so
 				// that each warp keeps two rows in flight; the adds stay in order
@@ -361,12 +367,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 		if (!ok && !first) continue;            // NaN already written by the first chunk
 		if (ok)
 		{
-			traverse(G, xs, lane, lo_n, hi_n, [&](unsigned mask, int n0, double w, const uint4& rec)
+			traverse(G, xs, lane, lo_n, hi_n, [&](unsigned mask, int n0, double w, const uint4& rec, float rm)
 			{
 				const bool mine = (mask >> lane) & 1u;
 				unsigned cm = __ballot_sync(FULL, mine && (rec.z & NODE_COARSE));
 				const uint32_t ci = ((cm >> lane) & 1u) ? __ldg(G.coarse_index + n0 + lane) : 0u;
-				unsigned fm = mask & ~cm;
+				// fine terms bounded below skip_below are dropped before their
+				// row is read
+				const unsigned sm = __ballot_sync(FULL, mine && (float)fabs(w) * rm < G.skip_below);
+				unsigned fm = mask & ~cm & ~sm;
 				while (cm)
 				{
 					const int k = __ffs(cm) - 1;
@@ -456,7 +465,7 @@ __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ Fw
 		const GridDesc& G = a.g[find_grid(a, p)];
 		long long cnt = 0;
 		if (load_point(a, p, xs, lane))
-			traverse(G, xs, lane, [&](unsigned mask, int, double, const uint4&) { cnt += __popc(mask); });
+			traverse(G, xs, lane, [&](unsigned mask, int, double, const uint4&, float) { cnt += __popc(mask); });
 		if (lane == 0) counts[p] = cnt;
 		__syncwarp();
 	}
@@ -510,7 +519,7 @@ __global__ void __launch_bounds__(BLOCK) bwd_points_kernel(const __grid_constant
 		}
 		__syncwarp();
 		long long woff = a.pair_off ? a.pair_off[p] : 0;
-		traverse(G, xs, lane, [&](unsigned mask, int n0, double w, const uint4& rec)
+		traverse(G, xs, lane, [&](unsigned mask, int n0, double w, const uint4& rec, float)
 		{
 			if (a.pair_off)
 			{
@@ -712,6 +721,8 @@ struct sgi_grid
 	int dim = 0, nno = 0, TD = 0, ld = 0;
 	uint4* rec = nullptr;
 	uint2* comps = nullptr;
+	float* rowmax = nullptr;
+	float skip_below = 0.f;
 	double* s64 = nullptr;
 	float* s32 = nullptr;
 	double* s64c = nullptr;
@@ -740,14 +751,19 @@ void free_grid(sgi_grid* g)
 	cudaSetDevice(g->device);
 	cudaFree(g->rec); cudaFree(g->comps); cudaFree(g->s64); cudaFree(g->s32); cudaFree(g->s64c); cudaFree(g->coarse_index);
 	cudaFree(g->parent);
+	cudaFree(g->rowmax);
 	cudaSetDevice(prev);
 	delete g;
 }
 
-GridDesc desc_of(const sgi_grid* g, long long pt_begin)
+// precision SGI_FP32C also hands the kernel the row maxima for its
+// negligible-term test; the FP64 form keeps every term.
+GridDesc desc_of(const sgi_grid* g, long long pt_begin, int precision = SGI_FP64)
 {
 	GridDesc d;
-	d.rec = g->rec; d.comps = g->comps; d.s64 = g->s64; d.s32 = g->s32; d.s64c = g->s64c;
+	d.rec = g->rec; d.comps = g->comps;
+	d.rowmax = precision == SGI_FP32C ? g->rowmax : nullptr;
+	d.skip_below = precision == SGI_FP32C ? g->skip_below : 0.f; d.s64 = g->s64; d.s32 = g->s32; d.s64c = g->s64c;
 	d.coarse_index = g->coarse_index; d.parent = g->parent; d.pt_begin = pt_begin; d.nno = g->nno; d.ld = g->ld;
 	return d;
 }
@@ -825,6 +841,20 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 			}
 		rc = upload((void**)&d->s32, hi.data(), hi.size() * 4);
 		if (!rc) rc = upload((void**)&d->s64c, coarse.data(), coarse.size() * 8);
+		// row maxima for the FP32C form's negligible-term test: a fine term is
+		// dropped when |w| * max|s_row| < 2^-46 * max|s| (at most ~2,000
+		// dropped terms per point: below 1e-10 of the largest surplus)
+		std::vector<float> rmax(nrow, 0.f);
+		double smax = 0.0;
+		for (int n = 0; n < g.nno; n++)
+		{
+			double m = 0.0;
+			for (int o = 0; o < g.TotalDof; o++) m = std::max(m, fabs(g.surplus[(size_t)n * g.TotalDof + o]));
+			rmax[n] = (float)(m * (1.0 + 0x1.0p-20));   // rounded up
+			smax = std::max(smax, m);
+		}
+		if (!rc) rc = upload((void**)&d->rowmax, rmax.data(), rmax.size() * 4);
+		d->skip_below = (float)(ldexp(smax, -46));
 	}
 	if (rc) { free_grid(d); return rc; }
 	sgi_grid_info& I = d->info;
@@ -904,7 +934,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 		if (p1 == p0) continue;
 		FwdArgs a;
 		memset(&a, 0, sizeof(a));
-		for (int k = 0; k < ng; k++) a.g[k] = desc_of(grids[gb + k], pt_offsets[gb + k] - p0);
+		for (int k = 0; k < ng; k++) a.g[k] = desc_of(grids[gb + k], pt_offsets[gb + k] - p0, precision);
 		a.x = x + (size_t)p0 * g0->dim;
 		a.out = out + (size_t)p0 * g0->TD;
 		a.npts = p1 - p0;
@@ -1202,7 +1232,7 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		if (p1 == p0) continue;
 		FwdArgs a;
 		memset(&a, 0, sizeof(a));
-		for (int k = 0; k < ng; k++) a.g[k] = desc_of(grids[gb + k], pt_offsets[gb + k] - p0);
+		for (int k = 0; k < ng; k++) a.g[k] = desc_of(grids[gb + k], pt_offsets[gb + k] - p0, precision);
 		a.x = x + (size_t)p0 * g0->dim;
 		a.out = out + (size_t)p0 * g0->TD;
 		a.npts = p1 - p0;
