@@ -376,23 +376,35 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 				// row is read
 				const unsigned sm = __ballot_sync(FULL, mine && (float)fabs(w) * rm < G.skip_below);
 				unsigned fm = mask & ~cm & ~sm;
+				// coarse hits two at a time (two FP64 rows in flight)
 				while (cm)
 				{
-					const int k = __ffs(cm) - 1;
+					const int k0 = __ffs(cm) - 1;
 					cm &= cm - 1;
-					const double wk = __shfl_sync(FULL, w, k);
-					const double* row = G.s64c + (size_t)__shfl_sync(FULL, ci, k) * G.ld + a.o_begin;
-					double sv[V][E];
+					const bool two = cm != 0u;
+					const int k1 = two ? __ffs(cm) - 1 : k0;
+					if (two) cm &= cm - 1;
+					const double w0 = __shfl_sync(FULL, w, k0);
+					const double w1 = __shfl_sync(FULL, w, k1);
+					const double* row0 = G.s64c + (size_t)__shfl_sync(FULL, ci, k0) * G.ld + a.o_begin;
+					const double* row1 = G.s64c + (size_t)__shfl_sync(FULL, ci, k1) * G.ld + a.o_begin;
+					double s0[V][E], s1[V][E];
 #pragma unroll
 					for (int v = 0; v < V; v++)
 					{
 						const int o = out_col<E>(v, lane);
-						load_row<E>(row, o, a.o_begin + o < G.ld, sv[v]);
+						const bool in = a.o_begin + o < G.ld;
+						load_row<E>(row0, o, in, s0[v]);
+						load_row<E>(row1, o, in && two, s1[v]);
 					}
 #pragma unroll
 					for (int v = 0; v < V; v++)
 #pragma unroll
-						for (int e = 0; e < E; e++) acc[v][e] = fma(wk, sv[v][e], acc[v][e]);
+						for (int e = 0; e < E; e++)
+						{
+							acc[v][e] = fma(w0, s0[v][e], acc[v][e]);
+							if (two) acc[v][e] = fma(w1, s1[v][e], acc[v][e]);
+						}
 				}
 				// Q rows in flight; each pair of hits is summed in FP32 and
 				// added to the FP64 running sum
@@ -638,7 +650,9 @@ struct DeviceWork
 	// host-pointer staging
 	double* dx = nullptr; size_t dx_bytes = 0;
 	double* dout = nullptr; size_t dout_bytes = 0;
-	cudaStream_t stream = nullptr;
+	cudaStream_t stream = nullptr, copy_in = nullptr, copy_out = nullptr;
+	static constexpr int NEV = 8;
+	cudaEvent_t ev_in[NEV] = {}, ev_done[NEV] = {};
 };
 constexpr unsigned NCOUNTERS = 1u << 16;
 
@@ -662,8 +676,8 @@ int device_work(int dev, DeviceWork** out)
 }
 
 // Node-range chunk for the forward launches: grids whose surplus rows exceed
-// half the L2 are walked in node ranges whose rows fit in that half, all
-// points per range, so that the rows each range gathers stay L2-resident.
+// the L2 are walked in node ranges, all points per range, so that the rows
+// each range gathers stay mostly L2-resident.
 // Small batches are not chunked.  sgi_set_chunk_rows (or SGI_CHUNK_ROWS at
 // start-up) overrides: 0 = no chunks, n > 0 = chunks of n nodes.
 std::atomic<int> g_chunk_override{[]() { const char* e = getenv("SGI_CHUNK_ROWS"); return e ? atoi(e) : -1; }()};
@@ -737,8 +751,11 @@ int chunk_rows(const DeviceWork* W, const sgi_grid* g0, int precision, long long
 {
 	const int env = chunk_rows_env();
 	if (env >= 0) return env >= maxnno ? 0 : env;
+	// rows filling one L2 (FP64) or two (FP32C, whose coarse rows and
+	// dropped terms leave part of each chunk unread): the autotuner's choice
+	// on the d=59, 1M-node, TotalDof=256 workload
 	const long long row = (long long)g0->ld * (precision == SGI_FP64 ? 8 : 4);
-	const long long rows = std::max(1024ll, (long long)W->l2_bytes / 2 / row);
+	const long long rows = std::max(1024ll, (long long)W->l2_bytes * (precision == SGI_FP64 ? 1 : 2) / row);
 	if (npts < 4096 || maxnno <= rows) return 0;
 	return (int)rows;
 }
@@ -1016,14 +1033,64 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 	rc = device_work(g0->device, &W);
 	if (rc) return rc;
 	std::lock_guard<std::mutex> lk(W->mtx);
-	if (!W->stream) CUDA_TRY(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
-	const size_t xb = (size_t)npts * g0->dim * sizeof(double), ob = (size_t)npts * g0->TD * sizeof(double);
+	if (!W->stream)
+	{
+		CUDA_TRY(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
+		CUDA_TRY(cudaStreamCreateWithFlags(&W->copy_in, cudaStreamNonBlocking));
+		CUDA_TRY(cudaStreamCreateWithFlags(&W->copy_out, cudaStreamNonBlocking));
+		for (int k = 0; k < DeviceWork::NEV; k++)
+		{
+			CUDA_TRY(cudaEventCreateWithFlags(&W->ev_in[k], cudaEventDisableTiming));
+			CUDA_TRY(cudaEventCreateWithFlags(&W->ev_done[k], cudaEventDisableTiming));
+		}
+	}
+	const int D = g0->dim, TD = g0->TD;
+	const size_t xb = (size_t)npts * D * sizeof(double), ob = (size_t)npts * TD * sizeof(double);
 	if (W->dx_bytes < xb) { cudaFree(W->dx); W->dx = nullptr; W->dx_bytes = 0; CUDA_TRY(cudaMalloc(&W->dx, xb)); W->dx_bytes = xb; }
 	if (W->dout_bytes < ob) { cudaFree(W->dout); W->dout = nullptr; W->dout_bytes = 0; CUDA_TRY(cudaMalloc(&W->dout, ob)); W->dout_bytes = ob; }
-	CUDA_TRY(cudaMemcpyAsync(W->dx, x, xb, cudaMemcpyHostToDevice, W->stream));
-	rc = launch_forward(ngrids, grids, pt_offsets, W->dx, W->dout, precision, W->stream);
-	if (rc) return rc;
-	CUDA_TRY(cudaMemcpyAsync(out, W->dout, ob, cudaMemcpyDeviceToHost, W->stream));
+	// With pinned host buffers the batch is cut into sub-batches whose copies
+	// in and out overlap the other sub-batches' kernels (three streams); with
+	// pageable buffers the copies would block the host, so it runs as one.
+	cudaPointerAttributes ax{}, ao{};
+	const bool pinned = cudaPointerGetAttributes(&ax, x) == cudaSuccess && ax.type == cudaMemoryTypeHost &&
+		cudaPointerGetAttributes(&ao, out) == cudaSuccess && ao.type == cudaMemoryTypeHost;
+	cudaGetLastError();
+	// two halves: every sub-batch repeats all node-chunk launches, so more
+	// sub-batches buy overlap with launch tails
+	const int nsub = !pinned ? 1 : npts >= 128 * 1024 ? 2 : 1;
+	std::vector<long long> cut(nsub + 1);
+	for (int b = 0; b <= nsub; b++) cut[b] = npts * b / nsub;
+	std::vector<sgi_grid_t> sg;
+	std::vector<long long> so;
+	for (int b = 0; b < nsub; b++)
+	{
+		const long long P0 = cut[b], P1 = cut[b + 1];
+		if (P1 == P0) continue;
+		cudaEvent_t ein = W->ev_in[b % DeviceWork::NEV], edone = W->ev_done[b % DeviceWork::NEV];
+		CUDA_TRY(cudaMemcpyAsync(W->dx + (size_t)P0 * D, x + (size_t)P0 * D, (size_t)(P1 - P0) * D * sizeof(double),
+			cudaMemcpyHostToDevice, W->copy_in));
+		CUDA_TRY(cudaEventRecord(ein, W->copy_in));
+		CUDA_TRY(cudaStreamWaitEvent(W->stream, ein, 0));
+		// the grids overlapping [P0, P1), offsets relative to P0
+		sg.clear();
+		so.clear();
+		for (int k = 0; k < ngrids; k++)
+		{
+			const long long lo = std::max(P0, pt_offsets[k]), hi = std::min(P1, pt_offsets[k + 1]);
+			if (hi <= lo) continue;
+			sg.push_back(grids[k]);
+			so.push_back(lo - P0);
+		}
+		so.push_back(P1 - P0);
+		rc = launch_forward((int)sg.size(), sg.data(), so.data(), W->dx + (size_t)P0 * D, W->dout + (size_t)P0 * TD,
+			precision, W->stream);
+		if (rc) return rc;
+		CUDA_TRY(cudaEventRecord(edone, W->stream));
+		CUDA_TRY(cudaStreamWaitEvent(W->copy_out, edone, 0));
+		CUDA_TRY(cudaMemcpyAsync(out + (size_t)P0 * TD, W->dout + (size_t)P0 * TD, (size_t)(P1 - P0) * TD * sizeof(double),
+			cudaMemcpyDeviceToHost, W->copy_out));
+	}
+	CUDA_TRY(cudaStreamSynchronize(W->copy_out));
 	CUDA_TRY(cudaStreamSynchronize(W->stream));
 	return SGI_OK;
 }

@@ -199,8 +199,8 @@ int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, const long long
 int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream);
 
 /* Node-range chunking of the forward launches (process-wide).  A grid whose
- * surplus rows exceed half the L2 is walked in chunks of consecutive nodes
- * whose rows fit there, every point against one chunk per launch, the outputs
+ * surplus rows exceed the L2 is walked in chunks of consecutive nodes (rows
+ * filling one L2 for FP64, two for FP32C), every point against one chunk per launch, the outputs
  * carried between chunks in FP64 (the FP64 form keeps gold's order and bits).
  * rows < 0: automatic (the default; batches under 4096 points are not
  * chunked); 0: never chunk; > 0: chunks of `rows` nodes.  Returns the previous

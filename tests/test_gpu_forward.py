@@ -259,3 +259,29 @@ def test_wide_component_form_bit_exact(cuda):
     ref = O.Gold(idx, sur).interpolate(X)
     assert np.array_equal(_run(g, X), ref)
     assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
+
+
+def test_host_entry_pipelined_sub_batches(cuda):
+    """Pinned host buffers with >= 128k points go through overlapped
+    copy-in / kernel / copy-out sub-batches; FP64 stays gold-exact."""
+    import ctypes
+    import torch
+    hosts = [H.HostGrid.adaptive(8, 3000, 40, seed=60), H.HostGrid.adaptive(8, 1500, 40, seed=61)]
+    grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
+    counts = [150_000, 60_000]
+    X = H.gen_points(8, sum(counts), kind=2, seed=62)
+    xh = torch.from_numpy(X).pin_memory()
+    outh = torch.zeros((sum(counts), 40), dtype=torch.float64).pin_memory()
+    offs = np.array([0, counts[0], sum(counts)], np.int64)
+    arr = (ctypes.c_void_p * 2)(grids[0].handle.value, grids[1].handle.value)
+    for precision in (H.FP64, H.FP32C):
+        rc = H.lib.sgi_interpolate_host(2, arr, offs.ctypes.data, xh.data_ptr(), outh.data_ptr(), precision)
+        assert rc == 0, H.lib.sgi_last_error().decode()
+        dev = _run(grids, X, precision, counts=counts)
+        if precision == H.FP64:
+            assert np.array_equal(outh.numpy(), dev)
+            sub = np.r_[0:150_000:997, 150_000:210_000:499]
+            for k, sl in ((0, sub[sub < 150_000]), (1, sub[sub >= 150_000])):
+                assert np.array_equal(dev[sl], O.Gold(*hosts[k].arrays()).interpolate(X[sl]))
+        else:
+            assert O.rel_error(outh.numpy(), dev)[0] <= 1e-9
