@@ -56,6 +56,7 @@ struct GridDesc
 	const uint32_t* coarse_index; // row of node n in s64c, for coarse nodes
 	const int* parent;           // tree parent per node (-1 for roots)
 	const float* rowmax;         // largest |surplus| of each row (FP32C), or null
+	const uint2* aux;            // {parent's component in the delta dim, depth}: FP32C weights
 	float skip_below;            // FP32C drops fine terms with |w| * rowmax below this
 	long long pt_begin;
 	int nno;
@@ -131,37 +132,64 @@ __device__ __forceinline__ bool node_active(const GridDesc& G, const double* xs,
 	return act;
 }
 
-template <class OnHits>
+// Depth of the per-warp weight stack of the incremental form.
+constexpr int WPATH = 64;
+
+// INCR (FP32C): a hit's weight is its tree parent's weight times its delta
+// hat over the parent's hat in that dimension (1 when the parent is constant
+// there).  A hit whose parent precedes the window reads the parent's weight
+// from wpath[depth - 1], the weight of the last hit one level up, which in
+// depth-first order is the parent; hits whose parent is in the same window
+// take it from that lane; wpath[0] = 1 stands for the roots' parent.  Chunk roots, nodes differing from
+// their parent in several dimensions and nodes deeper than the stack take the
+// full product.  Without INCR every hit takes the full product (the FP64 form:
+// gold's multiplies in gold's order).
+template <bool INCR, class OnHits>
 __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, int a, int b,
-	OnHits&& on_hits)
+	OnHits&& on_hits, double* wpath = nullptr)
 {
 	int n0 = a;
+	if (INCR)
+	{
+		if (lane == 0) wpath[0] = 1.0;
+		__syncwarp();
+	}
 	// the next window's records are fetched before this window's hits are
 	// accumulated, so that their latency overlaps the row gathers
 	uint4 rn = make_uint4(0u, 0u, 0u, 0u);
+	uint2 xn = make_uint2(0u, 0u);
 	int pn = -1;
 	float mn = 0.f;
 	if (n0 + lane < b)
 	{
 		rn = __ldg(G.rec + n0 + lane);
-		if (a > 0) pn = __ldg(G.parent + n0 + lane);
+		if (INCR || a > 0) pn = __ldg(G.parent + n0 + lane);
 		if (G.rowmax) mn = __ldg(G.rowmax + n0 + lane);
+		if (INCR) xn = __ldg(G.aux + n0 + lane);
 	}
 	while (n0 < b)
 	{
 		const int idx = n0 + lane;
 		const bool valid = idx < b;
 		const uint4 r = rn;
+		const uint2 ax = xn;
 		const float rm = mn;
 		const uint32_t ncomp = r.z & 0xffu;
 		const bool chunk_root = a > 0 && valid && pn < a;
-		bool act = false;
+		bool act = false, full = false;
+		double factor = 1.0;
 		if (valid)
 		{
 			if (r.z & NODE_DEAD) act = false;
-			else if ((r.z & NODE_MULTI) || chunk_root) act = node_active(G, xs, r.y, ncomp);
+			else if ((r.z & NODE_MULTI) || chunk_root) { act = node_active(G, xs, r.y, ncomp); full = true; }
 			else if (r.z & NODE_ALWAYS) act = true;
-			else act = hat(xs[r.z >> 16], r.w) > 0.0;
+			else
+			{
+				const double hd = hat(xs[r.z >> 16], r.w);
+				act = hd > 0.0;
+				if (INCR && act) factor = ax.x ? __dmul_rn(hd, __drcp_rn(hat(xs[r.z >> 16], ax.x))) : hd;
+			}
+			if (INCR && ax.y >= (uint32_t)WPATH) full = true;
 		}
 		const unsigned cover = (valid && !act) ? r.x : 0u;
 		unsigned inc = cover;
@@ -177,15 +205,38 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 		const unsigned mask = __ballot_sync(FULL, hit);
 		const unsigned last = __shfl_sync(FULL, inc, 31);
 		const int nnext = max(n0 + 32, (int)last);
+		const int pcur = pn;
 		rn = make_uint4(0u, 0u, 0u, 0u);
 		pn = -1;
 		if (nnext + lane < b)
 		{
 			rn = __ldg(G.rec + nnext + lane);
-			if (a > 0) pn = __ldg(G.parent + nnext + lane);
+			if (INCR || a > 0) pn = __ldg(G.parent + nnext + lane);
 			if (G.rowmax) mn = __ldg(G.rowmax + nnext + lane);
+			if (INCR) xn = __ldg(G.aux + nnext + lane);
 		}
-		const double w = hit ? node_weight(G, xs, r.y, ncomp) : 0.0;
+		double w = 0.0;
+		if (!INCR) w = hit ? node_weight(G, xs, r.y, ncomp) : 0.0;
+		else if (mask)
+		{
+			// hits whose parent precedes the window take its weight from the
+			// stack; chains of hits inside the window resolve in shuffle rounds
+			if (hit) w = full ? node_weight(G, xs, r.y, ncomp)
+			               : (pcur < n0 ? wpath[ax.y - 1] * factor : 0.0);
+			const int plane = pcur - n0;                 // parent's lane, if in the window
+			bool done = !hit || full || pcur < n0;
+			for (int round = 0; round < 32 && __any_sync(FULL, !done); round++)
+			{
+				const double wp = __shfl_sync(FULL, w, plane >= 0 && plane < 32 ? plane : lane);
+				const bool pdone = __shfl_sync(FULL, (int)done, plane >= 0 && plane < 32 ? plane : lane);
+				if (!done && pdone) { w = wp * factor; done = true; }
+			}
+			// the deepest-indexed hit at each depth becomes that depth's entry
+			__syncwarp();
+			const unsigned same = __match_any_sync(FULL, hit ? ax.y : 0xffffffffu);
+			if (hit && ax.y < (uint32_t)WPATH && (31 - __clz(same & mask)) == lane) wpath[ax.y] = w;
+			__syncwarp();
+		}
 		if (mask) on_hits(mask, n0, w, r, rm);
 		n0 = nnext;
 	}
@@ -194,7 +245,7 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 template <class OnHits>
 __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, OnHits&& on_hits)
 {
-	traverse(G, xs, lane, 0, G.nno, on_hits);
+	traverse<false>(G, xs, lane, 0, G.nno, on_hits);
 }
 
 // Node range of this launch for grid G.
@@ -281,7 +332,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 		if (!ok && !first) continue;        // NaN already written by the first chunk
 		if (ok)
 		{
-			traverse(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&, float)
+			traverse<false>(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&, float)
 			{
 				// two hits per step, both rows loaded before either is added, so
 				// that each warp keeps two rows in flight; the adds stay in order
@@ -331,17 +382,17 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 
 // FP32 + compensated form.  Rows are read in FP32, except the coarse rows
 // (largest |surplus| at least 2^-12 of the grid's largest), whose terms carry
-// most of the value and are read in FP64 and added with one FP64 FMA.  Other
-// hits are taken in pairs: each weight is split into FP32 hi and lo parts, the
-// pair's four FP32 products are summed in FP32 (the split keeps the weight's
-// rounding out of the result), and the pair sum is added to the output's FP64
-// running sum, which also carries the sums across node chunks.
+// most of the value and are read in FP64 and added with one FP64 FMA.  The
+// other ("fine") terms of a window, each bounded by 2^-12 of the largest
+// surplus, are summed in FP32 and the window's sum is added to the output's
+// FP64 running sum, which also carries the sums across node chunks.
 template <int V, int E, int Q, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_constant__ FwdArgs a)
 {
 	extern __shared__ double smem[];
 	const int lane = threadIdx.x & 31;
-	double* xs = smem + (threadIdx.x >> 5) * a.dim;
+	double* xs = smem + (threadIdx.x >> 5) * (a.dim + WPATH);
+	double* wpath = xs + a.dim;
 	const bool first = a.chunk_begin == 0;
 	for (;;)
 	{
@@ -367,7 +418,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 		if (!ok && !first) continue;            // NaN already written by the first chunk
 		if (ok)
 		{
-			traverse(G, xs, lane, lo_n, hi_n, [&](unsigned mask, int n0, double w, const uint4& rec, float rm)
+			traverse<true>(G, xs, lane, lo_n, hi_n, [&](unsigned mask, int n0, double w, const uint4& rec, float rm)
 			{
 				const bool mine = (mask >> lane) & 1u;
 				unsigned cm = __ballot_sync(FULL, mine && (rec.z & NODE_COARSE));
@@ -406,48 +457,50 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 							if (two) acc[v][e] = fma(w1, s1[v][e], acc[v][e]);
 						}
 				}
-				// Q rows in flight; each pair of hits is summed in FP32 and
-				// added to the FP64 running sum
-				while (fm)
+				// Q rows in flight; a window's fine terms are summed in FP32 and
+				// the sum is added to the FP64 running sum once per window
+				if (fm)
 				{
-					int k[Q];
-					float wh[Q], wl[Q];
-					const float* row[Q];
-#pragma unroll
-					for (int q = 0; q < Q; q++)
-					{
-						const bool have = fm != 0u;
-						k[q] = have ? __ffs(fm) - 1 : 0;
-						if (have) fm &= fm - 1;
-						const double wq = have ? __shfl_sync(FULL, w, k[q]) : 0.0;
-						wh[q] = __double2float_rn(wq);
-						wl[q] = __double2float_rn(wq - (double)wh[q]);
-						row[q] = G.s32 + (size_t)(n0 + k[q]) * G.ld + a.o_begin;
-					}
-					float sv[Q][V][E];
-#pragma unroll
-					for (int v = 0; v < V; v++)
-					{
-						const int o = out_col<E>(v, lane);
-						const bool in = a.o_begin + o < G.ld;
-#pragma unroll
-						for (int q = 0; q < Q; q++) load_row<E>(row[q], o, in, sv[q][v]);
-					}
+					float part[V][E];
 #pragma unroll
 					for (int v = 0; v < V; v++)
 #pragma unroll
-						for (int e = 0; e < E; e++)
+						for (int e = 0; e < E; e++) part[v][e] = 0.f;
+					while (fm)
+					{
+						float wf[Q];
+						const float* row[Q];
 #pragma unroll
-							for (int q = 0; q < Q; q += 2)
-							{
-								float f = __fmul_rn(wl[q], sv[q][v][e]);
-								f = __fmaf_rn(wl[q + 1], sv[q + 1][v][e], f);
-								f = __fmaf_rn(wh[q + 1], sv[q + 1][v][e], f);
-								f = __fmaf_rn(wh[q], sv[q][v][e], f);
-								acc[v][e] = __dadd_rn(acc[v][e], (double)f);
-							}
+						for (int q = 0; q < Q; q++)
+						{
+							const bool have = fm != 0u;
+							const int k = have ? __ffs(fm) - 1 : 0;
+							if (have) fm &= fm - 1;
+							wf[q] = have ? __double2float_rn(__shfl_sync(FULL, w, k)) : 0.f;
+							row[q] = G.s32 + (size_t)(n0 + k) * G.ld + a.o_begin;
+						}
+						float sv[Q][V][E];
+#pragma unroll
+						for (int v = 0; v < V; v++)
+						{
+							const int o = out_col<E>(v, lane);
+							const bool in = a.o_begin + o < G.ld;
+#pragma unroll
+							for (int q = 0; q < Q; q++) load_row<E>(row[q], o, in, sv[q][v]);
+						}
+#pragma unroll
+						for (int v = 0; v < V; v++)
+#pragma unroll
+							for (int e = 0; e < E; e++)
+#pragma unroll
+								for (int q = 0; q < Q; q++) part[v][e] = __fmaf_rn(wf[q], sv[q][v][e], part[v][e]);
+					}
+#pragma unroll
+					for (int v = 0; v < V; v++)
+#pragma unroll
+						for (int e = 0; e < E; e++) acc[v][e] = __dadd_rn(acc[v][e], (double)part[v][e]);
 				}
-			});
+			}, wpath);
 		}
 #pragma unroll
 		for (int v = 0; v < V; v++)
@@ -737,6 +790,7 @@ struct sgi_grid
 	uint2* comps = nullptr;
 	float* rowmax = nullptr;
 	float skip_below = 0.f;
+	uint2* aux = nullptr;
 	double* s64 = nullptr;
 	float* s32 = nullptr;
 	double* s64c = nullptr;
@@ -769,6 +823,7 @@ void free_grid(sgi_grid* g)
 	cudaFree(g->rec); cudaFree(g->comps); cudaFree(g->s64); cudaFree(g->s32); cudaFree(g->s64c); cudaFree(g->coarse_index);
 	cudaFree(g->parent);
 	cudaFree(g->rowmax);
+	cudaFree(g->aux);
 	cudaSetDevice(prev);
 	delete g;
 }
@@ -780,6 +835,7 @@ GridDesc desc_of(const sgi_grid* g, long long pt_begin, int precision = SGI_FP64
 	GridDesc d;
 	d.rec = g->rec; d.comps = g->comps;
 	d.rowmax = precision == SGI_FP32C ? g->rowmax : nullptr;
+	d.aux = g->aux;
 	d.skip_below = precision == SGI_FP32C ? g->skip_below : 0.f; d.s64 = g->s64; d.s32 = g->s32; d.s64c = g->s64c;
 	d.coarse_index = g->coarse_index; d.parent = g->parent; d.pt_begin = pt_begin; d.nno = g->nno; d.ld = g->ld;
 	return d;
@@ -871,6 +927,7 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 			smax = std::max(smax, m);
 		}
 		if (!rc) rc = upload((void**)&d->rowmax, rmax.data(), rmax.size() * 4);
+		if (!rc) rc = upload((void**)&d->aux, L.aux.data(), L.aux.size() * 4);
 		d->skip_below = (float)(ldexp(smax, -46));
 	}
 	if (rc) { free_grid(d); return rc; }
@@ -940,7 +997,8 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 	if (precision == SGI_FP64) { for (int k = 0; k < ngrids; k++) if (!grids[k]->s64) return fail(SGI_E_INVALID, "grid %d has no FP64 surplus", k); }
 	else if (precision == SGI_FP32C) { for (int k = 0; k < ngrids; k++) if (!grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k); }
 	else return fail(SGI_E_INVALID, "unknown precision %d", precision);
-	const size_t smem = (size_t)WARPS * g0->dim * sizeof(double);
+	// per warp: the point's coordinates, and for FP32C the weight stack
+	const size_t smem = (size_t)WARPS * (g0->dim + (precision == SGI_FP32C ? WPATH : 0)) * sizeof(double);
 	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	g_stats = sgi_launch_stats{};
 	int launches = 0;
@@ -1273,7 +1331,7 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		if (precision == SGI_FP32C && !grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k);
 	}
 	const sgi_grid* g0 = grids[0];
-	const size_t smem = (size_t)WARPS * g0->dim * sizeof(double);
+	const size_t smem = (size_t)WARPS * (g0->dim + (precision == SGI_FP32C ? WPATH : 0)) * sizeof(double);
 	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	// count the launches first: reject before launching anything
 	const int passes = (g0->TD + PASS - 1) / PASS;

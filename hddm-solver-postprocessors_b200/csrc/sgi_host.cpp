@@ -797,7 +797,7 @@ int build_layout(const HostGrid& g, DeviceLayout& L)
 	// containment tree over the grid order: parent = deepest enclosing node
 	// still open on the stack; a node's subtree ends where it is popped
 	std::vector<int> stack, parent(nno, -1);
-	std::vector<uint32_t> skip(nno, 0);
+	std::vector<uint32_t> skip(nno, 0), depth(nno, 0);
 	L.tree_depth = 0; L.tree_roots = 0; L.multi_delta = 0;
 	for (int n = 0; n < nno; n++)
 	{
@@ -806,6 +806,7 @@ int build_layout(const HostGrid& g, DeviceLayout& L)
 		parent[n] = stack.empty() ? -1 : stack.back();
 		if (parent[n] < 0) L.tree_roots++;
 		stack.push_back(n);
+		depth[n] = (uint32_t)stack.size();
 		L.tree_depth = std::max(L.tree_depth, (int)stack.size());
 	}
 	for (int t : stack) skip[t] = nno;
@@ -820,6 +821,7 @@ int build_layout(const HostGrid& g, DeviceLayout& L)
 		if (m >= L.coarse_threshold && m > 0.0) L.lo_index[n] = (uint32_t)L.ncoarse++;
 	}
 	// records
+	L.aux.assign((size_t)2 * nno, 0u);
 	for (int n = 0; n < nno; n++)
 	{
 		const uint32_t cnt = cptr[n + 1] - cptr[n];
@@ -840,6 +842,13 @@ int build_layout(const HostGrid& g, DeviceLayout& L)
 			else if (ndelta > 1) { flags |= NODE_MULTI; L.multi_delta++; }
 		}
 		if (L.lo_index[n] != ~0u) flags |= NODE_COARSE;
+		// the parent's component in the delta dimension
+		uint32_t old = 0;
+		if (parent[n] >= 0 && !(flags & (NODE_DEAD | NODE_MULTI | NODE_ALWAYS)))
+			for (uint32_t b2 = cptr[parent[n]]; b2 < cptr[parent[n] + 1]; b2++)
+				if (C[2 * b2] == ddim) old = C[2 * b2 + 1];
+		L.aux[2 * (size_t)n + 0] = old;
+		L.aux[2 * (size_t)n + 1] = depth[n];
 		L.rec[4 * (size_t)n + 0] = skip[n];
 		L.rec[4 * (size_t)n + 1] = cptr[n];
 		L.rec[4 * (size_t)n + 2] = cnt | flags | (ddim << 16);

@@ -46,6 +46,10 @@ struct DeviceLayout
 	std::vector<uint32_t> comps; // 2 * ncomps
 	std::vector<uint32_t> lo_index; // nno: row in the lo array, or ~0u
 	std::vector<int> parent;        // nno: tree parent, or -1
+	// nno pairs {old, depth}: the parent's (i | j << 16) in the node's delta
+	// dimension (0 when the parent is constant there) and the node's tree
+	// depth (roots 1); the FP32C form builds weights along the tree from them
+	std::vector<uint32_t> aux;
 	int max_comps = 0, tree_depth = 0, tree_roots = 0, multi_delta = 0, ncoarse = 0;
 	double coarse_threshold = 0.0;
 };
