@@ -70,6 +70,32 @@ def alg_bytes(hg, info, npts, s_b):
             + 2 * info.nno * info.max_comps + 4 * szxps), szxps
 
 
+# Random 1 KB row gathers from an L2-resident region measured 18.2G rows/s
+# (18.7 TB/s) on this pool's B200s with 16-byte loads at 32 warps per SM
+# (profiles/gather_roof_probe.md): the roof of a kernel whose work is one row
+# gather per (point, active node) pair.
+GATHER_PEAK_TBS = 18.7
+
+# DRAM bytes (read + write) of one FP32C step of the default workload: the sum
+# over the four fwd_f32c_kernel launches of one graph replay in an ncu capture
+# (profiles/fwd_f32c_c4_traffic.md).
+FP32C_STEP_DRAM_BYTES = 270.2e9
+
+
+def gather_roof(mean_active, ms, grid, hg):
+    """Row bytes the FP32C step gathers (coarse rows FP64, others FP32, per
+    active pair) over the step time, against the measured gather peak."""
+    info = grid.info
+    row32 = info.ld * 4
+    bytes_per_pair = row32  # lower bound: every pair reads at least its FP32 row
+    b = mean_active * NPTS * bytes_per_pair
+    ach = b / (ms * 1e-3) / 1e12
+    return {"bound": "l2_gather", "achieved": ach, "peak": GATHER_PEAK_TBS, "unit": "TB/s",
+            "frac": ach / GATHER_PEAK_TBS, "bytes_per_pair": bytes_per_pair,
+            "note": "one FP32 row (TotalDof x 4 B) per active (point, node) pair over the step time; coarse "
+                    "rows read 2x that and dropped terms read none"}
+
+
 class Clocks:
     """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
 
@@ -158,6 +184,17 @@ def run_gpu(args):
         total = ev[0].elapsed_time(ev[steps])
         return total, per, plan.launches
 
+    if args.profile_replay:
+        # one warm-up and one measured replay of the FP32C plan (the timed
+        # step), nothing else: the case a launch-level capture looks at
+        chunk = args.chunk_rows if args.chunk_rows >= 0 else 259072
+        plan = H.Plan(grid, x, out32, precision=H.FP32C, chunk_rows=chunk, stream=stream)
+        plan.launch(stream=stream)
+        plan.launch(stream=stream)
+        torch.cuda.synchronize(dev)
+        print(json.dumps({"profile_replay": {"chunk_rows": plan.chunk_rows, "variant": plan.variant,
+                                             "launches": plan.launches}}))
+        return
     # accuracy of the FP32C form against the FP64 form (bit-identical to gold), all points
     H.interpolate(grid, x, precision=H.FP64, out=out64, stream=stream)
     H.interpolate(grid, x, precision=H.FP32C, out=out32, stream=stream)
@@ -230,10 +267,7 @@ def run_gpu(args):
         ach = b32 / (ms32 * 1e-3) / 1e9
         pts_s = npts * world / (ms32 * 1e-3)
         pts64_s = npts * world / (ms64 * 1e-3)
-        traffic = None
-        tf = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tf):
-            traffic = json.load(open(tf)).get("fwd_f32c_bytes_per_launch")
+        traffic = FP32C_STEP_DRAM_BYTES if npts == NPTS else None
         result = {
             "metric": METRIC,
             "value": pts_s,
@@ -260,6 +294,7 @@ def run_gpu(args):
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                          "peak_kind": f"{peak_kind} (burst copy)", "algorithmic_bytes_per_launch": b32,
                          "traffic": traffic, "kernel": "fwd_f32c_kernel"},
+            "gather_roofline": gather_roof(mean_active, ms32, grid, hg),
             "walk_only_ms": walk_ms,
             "fma_work": {"mean_active_nodes": mean_active,
                          "flops_per_launch": 2.0 * mean_active * TD * npts,
@@ -397,6 +432,28 @@ def run_c2(args):
                       "fp32c_vs_gold_exact_fp64": {"max_rel_err": emax, "rms_rel_err": erms}}))
 
 
+def run_chunksweep(args):
+    """Step time of both forms over fixed node-chunk sizes (the autotuner's
+    search space, printed), default workload."""
+    import torch
+    import hddm_b200 as H
+    dev = torch.device("cuda", 0)
+    hg, X, _ = make_workload(npts=args.points)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    x = torch.from_numpy(X).to(dev)
+    out = torch.empty((X.shape[0], TD), dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream(dev)
+    rows_list = [0, 32768, 49152, 65536, 98304, 131072, 196608, 262144]
+    res = {}
+    for prec, name in ((H.FP32C, "fp32c"), (H.FP64, "fp64")):
+        for rows in rows_list:
+            p = H.Plan(g, x, out, precision=prec, chunk_rows=rows, stream=s)
+            res.setdefault(name, []).append({"chunk_rows": rows, "launches": p.launches,
+                                             "ms": _plan_time(H, torch, p, s, 3, 2)})
+            del p
+    print(json.dumps({"workload": WORKLOAD, "chunk_sweep": res}))
+
+
 def run_c3(args):
     """Backward: d=59 adaptive grid of 300k nodes, TotalDof=128, 32768 points kept 1e-6
     from every kink; dL/dx and dL/dsurplus of L = sum c * f with c ~ N(0,1)."""
@@ -472,13 +529,15 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate"],
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "chunksweep"],
                     help="c4 (default) is the benchmark line; the others print their own measurements")
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=NPTS, help="points per GPU (default: the workload's 1M)")
     ap.add_argument("--chunk-rows", type=int, default=-1, help="node-chunk size of the plans (-1: autotune)")
+    ap.add_argument("--profile-replay", action="store_true",
+                    help="only run two replays of the FP32C plan (launch-level profiling case)")
     ap.add_argument("--only-accuracy-pass", action="store_true",
                     help="run one FP64 and one FP32C launch, print their agreement and exit (profiling case)")
     args = ap.parse_args()
@@ -492,6 +551,8 @@ def main():
         run_c3(args)
     elif args.workload == "multistate":
         run_multistate(args)
+    elif args.workload == "chunksweep":
+        run_chunksweep(args)
     else:
         run_gpu(args)
 
