@@ -83,8 +83,8 @@ FP32C_STEP_DRAM_BYTES = 270.2e9
 
 
 def gather_roof(mean_active, ms, grid, hg):
-    """Row bytes the FP32C step gathers (coarse rows FP64, others FP32, per
-    active pair) over the step time, against the measured gather peak."""
+    """Row bytes the FP32C step gathers (one FP32 row per active pair, a lower
+    bound) over the step time, against the measured gather peak."""
     info = grid.info
     row32 = info.ld * 4
     bytes_per_pair = row32  # lower bound: every pair reads at least its FP32 row
@@ -92,8 +92,8 @@ def gather_roof(mean_active, ms, grid, hg):
     ach = b / (ms * 1e-3) / 1e12
     return {"bound": "l2_gather", "achieved": ach, "peak": GATHER_PEAK_TBS, "unit": "TB/s",
             "frac": ach / GATHER_PEAK_TBS, "bytes_per_pair": bytes_per_pair,
-            "note": "one FP32 row (TotalDof x 4 B) per active (point, node) pair over the step time; coarse "
-                    "rows read 2x that and dropped terms read none"}
+            "note": "one FP32 row (TotalDof x 4 B) per active (point, node) pair over the step time; big "
+                    "terms read their FP64 row (2x) and dropped terms read none"}
 
 
 class Clocks:
@@ -454,6 +454,40 @@ def run_chunksweep(args):
     print(json.dumps({"workload": WORKLOAD, "chunk_sweep": res}))
 
 
+def run_variantsweep(args):
+    """FP32C step time of every kernel variant over node-chunk sizes (direct
+    calls, CUDA events), with each variant's error against the gold-exact FP64
+    form, default workload."""
+    import torch
+    import hddm_b200 as H
+    dev = torch.device("cuda", 0)
+    hg, X, _ = make_workload(npts=args.points)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    x = torch.from_numpy(X).to(dev)
+    ref = H.interpolate(g, x, precision=H.FP64)
+    rows_list = [int(r) for r in args.sweep_rows.split(",")]
+    res = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for v in [int(k) for k in args.sweep_variants.split(",")]:
+        H.set_fp32c_variant(v)
+        for rows in rows_list:
+            H.set_chunk_rows(rows)
+            out = H.interpolate(g, x, precision=H.FP32C)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(3):
+                H.interpolate(g, x, precision=H.FP32C, out=out)
+            e1.record()
+            torch.cuda.synchronize()
+            emax, erms = _rel_err(torch, out, ref)
+            res.append({"variant": v, "chunk_rows": rows, "ms": e0.elapsed_time(e1) / 3,
+                        "max_rel_err": emax, "rms_rel_err": erms})
+            print(json.dumps(res[-1]), file=sys.stderr)
+    H.set_fp32c_variant(-1)
+    H.set_chunk_rows(-1)
+    print(json.dumps({"workload": WORKLOAD, "variant_sweep": res}))
+
+
 def run_c3(args):
     """Backward: d=59 adaptive grid of 300k nodes, TotalDof=128, 32768 points kept 1e-6
     from every kink; dL/dx and dL/dsurplus of L = sum c * f with c ~ N(0,1)."""
@@ -529,9 +563,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "chunksweep"],
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "chunksweep", "variantsweep"],
                     help="c4 (default) is the benchmark line; the others print their own measurements")
     ap.add_argument("--cpu-sample", type=int, default=256)
+    ap.add_argument("--sweep-variants", default="0,1,2", help="variantsweep: FP32C variants")
+    ap.add_argument("--sweep-rows", default="0,131072,196608,262144,393216", help="variantsweep: chunk sizes")
     ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=NPTS, help="points per GPU (default: the workload's 1M)")
@@ -553,6 +589,8 @@ def main():
         run_multistate(args)
     elif args.workload == "chunksweep":
         run_chunksweep(args)
+    elif args.workload == "variantsweep":
+        run_variantsweep(args)
     else:
         run_gpu(args)
 

@@ -58,6 +58,7 @@ struct GridDesc
 	const float* rowmax;         // largest |surplus| of each row (FP32C), or null
 	const uint2* aux;            // {parent's component in the delta dim, depth}: FP32C weights
 	float skip_below;            // FP32C drops fine terms with |w| * rowmax below this
+	float big_below;             // FP32C list form: terms with |w| * rowmax from this up are big
 	long long pt_begin;
 	int nno;
 	int ld;
@@ -76,10 +77,28 @@ struct FwdArgs
 	int chunk_begin, chunk_len;
 };
 
+// Exact conversion of v < 2^32 to double in the FP64 pipe: the bit pattern
+// 0x43300000:v is 2^52 + v, and subtracting 2^52 is exact.
+__device__ __forceinline__ double u32_to_double(uint32_t v)
+{
+	return __dsub_rn(__hiloint2double(0x43300000, (int)v), 4503599627370496.0);
+}
+
 __device__ __forceinline__ double hat(double x, uint32_t ij)
 {
-	// 1 - |x*i - j| with the gold macro's rounding (LinearBasis/include/LinearBasis.h:50)
-	return __dsub_rn(1.0, fabs(__dsub_rn(__dmul_rn(x, (double)(ij & 0xffffu)), (double)(ij >> 16))));
+	// 1 - |x*i - j| with the gold macro's rounding (LinearBasis/include/LinearBasis.h:50);
+	// i and j convert exactly, so the result is the same as with (double)i, (double)j
+	return __dsub_rn(1.0, fabs(__dsub_rn(__dmul_rn(x, u32_to_double(ij & 0xffffu)), u32_to_double(ij >> 16))));
+}
+
+// 1/h for h in (0, 1], to about 2^-44 relative: the approximate FP64
+// reciprocal refined by one Newton-Raphson step, r' = r + r(1 - h r).
+__device__ __forceinline__ double rcp_weight(double h)
+{
+	double r;
+	asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(h));
+	const double e = fma(-h, r, 1.0);
+	return fma(r, e, r);
 }
 
 __device__ __forceinline__ int find_grid(const FwdArgs& a, long long p)
@@ -89,12 +108,6 @@ __device__ __forceinline__ int find_grid(const FwdArgs& a, long long p)
 	return gi;
 }
 
-// Walks nodes [a, b) of one grid for the point whose coordinates are in xs
-// (shared memory).  Calls on_hits(mask, n0, w, rec) per window; bits of mask
-// are hit lanes, lane k's w is the weight of node n0+k and rec its record.
-// A node whose tree parent lies before `a` ("chunk root") is checked on all its
-// components, since its ancestors are not walked; inside the range a node is
-// reached only when all its ancestors in the range are active.
 // Product of a hit node's hats in dimension order (the gold loop's `temp`).
 // Components are fetched four at a time, so a node costs one memory round
 // trip per four components instead of one per component.
@@ -135,15 +148,27 @@ __device__ __forceinline__ bool node_active(const GridDesc& G, const double* xs,
 // Depth of the per-warp weight stack of the incremental form.
 constexpr int WPATH = 64;
 
+// Walks nodes [a, b) of one grid for the point whose coordinates are in xs
+// (shared memory).  Calls on_hits(mask, n0, w, rec, rowmax) per window; bits
+// of mask are hit lanes, lane k's w is the weight of node n0+k, rec its record
+// and rowmax its row's largest |surplus| (when the grid descriptor has them).
+// A failing lane marks the lanes inside its subtree with a bit mask, and one
+// warp OR reduction gives every lane whether an earlier failing node covers
+// it; the next window starts at the larger of n0+32 and the largest failing
+// skip (one warp max reduction).
+// A node whose tree parent lies before `a` ("chunk root") is checked on all its
+// components, since its ancestors are not walked; inside the range a node is
+// reached only when all its ancestors in the range are active.
+// Without INCR every hit takes the full product (the FP64 form: gold's
+// multiplies in gold's order).
 // INCR (FP32C): a hit's weight is its tree parent's weight times its delta
 // hat over the parent's hat in that dimension (1 when the parent is constant
 // there).  A hit whose parent precedes the window reads the parent's weight
 // from wpath[depth - 1], the weight of the last hit one level up, which in
 // depth-first order is the parent; hits whose parent is in the same window
-// take it from that lane; wpath[0] = 1 stands for the roots' parent.  Chunk roots, nodes differing from
-// their parent in several dimensions and nodes deeper than the stack take the
-// full product.  Without INCR every hit takes the full product (the FP64 form:
-// gold's multiplies in gold's order).
+// take it from that lane; wpath[0] = 1 stands for the roots' parent.  Chunk
+// roots, nodes differing from their parent in several dimensions and nodes
+// deeper than the stack take the full product.
 template <bool INCR, class OnHits>
 __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, int a, int b,
 	OnHits&& on_hits, double* wpath = nullptr)
@@ -185,26 +210,25 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 			else if (r.z & NODE_ALWAYS) act = true;
 			else
 			{
-				const double hd = hat(xs[r.z >> 16], r.w);
+				const double xd = xs[r.z >> 16];
+				const double hd = hat(xd, r.w);
 				act = hd > 0.0;
-				if (INCR && act) factor = ax.x ? __dmul_rn(hd, __drcp_rn(hat(xs[r.z >> 16], ax.x))) : hd;
+				if (INCR && act) factor = ax.x ? hd * rcp_weight(hat(xd, ax.x)) : hd;
 			}
 			if (INCR && ax.y >= (uint32_t)WPATH) full = true;
 		}
+		// lanes lane+1 .. skip-n0-1 lie in a failing node's subtree
 		const unsigned cover = (valid && !act) ? r.x : 0u;
-		unsigned inc = cover;
-#pragma unroll
-		for (int off = 1; off < 32; off <<= 1)
+		unsigned bits = 0u;
+		if (cover)
 		{
-			const unsigned v = __shfl_up_sync(FULL, inc, off);
-			if (lane >= off) inc = max(inc, v);
+			const int e = min((int)cover - n0, 32);
+			bits = (e >= 32 ? FULL : ((1u << e) - 1u)) & ~((2u << lane) - 1u);
 		}
-		unsigned exc = __shfl_up_sync(FULL, inc, 1);
-		if (lane == 0) exc = 0u;
-		const bool hit = act && exc <= (unsigned)idx;
+		const unsigned pruned = __reduce_or_sync(FULL, bits);
+		const bool hit = act && !((pruned >> lane) & 1u);
 		const unsigned mask = __ballot_sync(FULL, hit);
-		const unsigned last = __shfl_sync(FULL, inc, 31);
-		const int nnext = max(n0 + 32, (int)last);
+		const int nnext = max(n0 + 32, (int)__reduce_max_sync(FULL, cover));
 		const int pcur = pn;
 		rn = make_uint4(0u, 0u, 0u, 0u);
 		pn = -1;
@@ -280,7 +304,13 @@ __device__ __forceinline__ int out_col(int v, int lane) { return v * 32 * E + la
 template <int E>
 __device__ __forceinline__ void load_row(const double* row, int o, bool in, double* d)
 {
-	if (E == 2)
+	if (E == 4)
+	{
+		const double2 t0 = in ? __ldg(reinterpret_cast<const double2*>(row + o)) : make_double2(0.0, 0.0);
+		const double2 t1 = in ? __ldg(reinterpret_cast<const double2*>(row + o + 2)) : make_double2(0.0, 0.0);
+		d[0] = t0.x; d[1] = t0.y; d[2] = t1.x; d[3] = t1.y;
+	}
+	else if (E == 2)
 	{
 		const double2 t = in ? __ldg(reinterpret_cast<const double2*>(row + o)) : make_double2(0.0, 0.0);
 		d[0] = t.x; d[1] = t.y;
@@ -291,7 +321,12 @@ __device__ __forceinline__ void load_row(const double* row, int o, bool in, doub
 template <int E>
 __device__ __forceinline__ void load_row(const float* row, int o, bool in, float* d)
 {
-	if (E == 2)
+	if (E == 4)
+	{
+		const float4 t = in ? __ldg(reinterpret_cast<const float4*>(row + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
+		d[0] = t.x; d[1] = t.y; d[2] = t.z; d[3] = t.w;
+	}
+	else if (E == 2)
 	{
 		const float2 t = in ? __ldg(reinterpret_cast<const float2*>(row + o)) : make_float2(0.f, 0.f);
 		d[0] = t.x; d[1] = t.y;
@@ -380,19 +415,37 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 	}
 }
 
-// FP32 + compensated form.  Rows are read in FP32, except the coarse rows
-// (largest |surplus| at least 2^-12 of the grid's largest), whose terms carry
-// most of the value and are read in FP64 and added with one FP64 FMA.  The
-// other ("fine") terms of a window, each bounded by 2^-12 of the largest
-// surplus, are summed in FP32 and the window's sum is added to the output's
-// FP64 running sum, which also carries the sums across node chunks.
+// Per-warp list of fine terms, {row, FP32 weight}: a window's fine hits are
+// appended, and the list is drained once it holds 32 or more.
+constexpr int FCAP = 64;
+
+// Shared memory per warp of the list form, in doubles: the list, the weight
+// stack and the point (rounded up to keep the next warp 16-byte aligned).
+__host__ __device__ __forceinline__ int list_stride(int dim) { return FCAP + WPATH + ((dim + 1) & ~1); }
+
+// FP32 + compensated form.  Terms are split by size: a term is "big" when
+// |w| * max|s_row| is at least the coarse threshold (2^-16 of the largest
+// surplus by default); big terms read the FP64 copy of their row (rows whose
+// largest |surplus| reaches the threshold have one) and add with an FP64 FMA.
+// The other ("fine") terms, each below the threshold, are appended to a
+// per-warp list of {row, FP32 weight} entries and gathered in FP32 in groups
+// of Q rows; their FP32 partial sums are added to the outputs' FP64 running
+// sums every FLUSH terms.  Fine terms below 2^-46 of the largest surplus are
+// dropped before their row is read.  The running sums also carry the outputs
+// across node chunks.
+constexpr int FLUSH = 8;
+
 template <int V, int E, int Q, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_constant__ FwdArgs a)
 {
+	static_assert(FLUSH % Q == 0 || Q % FLUSH == 0, "groups of Q must tile the flush interval");
+	static_assert(32 % Q == 0, "groups of Q must tile a window");
 	extern __shared__ double smem[];
 	const int lane = threadIdx.x & 31;
-	double* xs = smem + (threadIdx.x >> 5) * (a.dim + WPATH);
-	double* wpath = xs + a.dim;
+	double* wbase = smem + (threadIdx.x >> 5) * list_stride(a.dim);
+	uint2* fl = reinterpret_cast<uint2*>(wbase);
+	double* wpath = wbase + FCAP;
+	double* xs = wpath + WPATH;
 	const bool first = a.chunk_begin == 0;
 	for (;;)
 	{
@@ -418,89 +471,129 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 		if (!ok && !first) continue;            // NaN already written by the first chunk
 		if (ok)
 		{
-			traverse<true>(G, xs, lane, lo_n, hi_n, [&](unsigned mask, int n0, double w, const uint4& rec, float rm)
-			{
-				const bool mine = (mask >> lane) & 1u;
-				unsigned cm = __ballot_sync(FULL, mine && (rec.z & NODE_COARSE));
-				const uint32_t ci = ((cm >> lane) & 1u) ? __ldg(G.coarse_index + n0 + lane) : 0u;
-				// fine terms bounded below skip_below are dropped before their
-				// row is read
-				const unsigned sm = __ballot_sync(FULL, mine && (float)fabs(w) * rm < G.skip_below);
-				unsigned fm = mask & ~cm & ~sm;
-				// coarse hits two at a time (two FP64 rows in flight)
-				while (cm)
-				{
-					const int k0 = __ffs(cm) - 1;
-					cm &= cm - 1;
-					const bool two = cm != 0u;
-					const int k1 = two ? __ffs(cm) - 1 : k0;
-					if (two) cm &= cm - 1;
-					const double w0 = __shfl_sync(FULL, w, k0);
-					const double w1 = __shfl_sync(FULL, w, k1);
-					const double* row0 = G.s64c + (size_t)__shfl_sync(FULL, ci, k0) * G.ld + a.o_begin;
-					const double* row1 = G.s64c + (size_t)__shfl_sync(FULL, ci, k1) * G.ld + a.o_begin;
-					double s0[V][E], s1[V][E];
+			const int lcol = a.o_begin + out_col<E>(0, lane);
+			const float* s32l = G.s32 + lcol;
+			const double* s64l = G.s64c + lcol;
+			const uint32_t ld = (uint32_t)G.ld;
+			float part[V][E];
 #pragma unroll
-					for (int v = 0; v < V; v++)
+			for (int v = 0; v < V; v++)
+#pragma unroll
+				for (int e = 0; e < E; e++) part[v][e] = 0.f;
+			int cnt = 0, since = 0;
+			auto flush = [&]()
+			{
+#pragma unroll
+				for (int v = 0; v < V; v++)
+#pragma unroll
+					for (int e = 0; e < E; e++) { acc[v][e] = __dadd_rn(acc[v][e], (double)part[v][e]); part[v][e] = 0.f; }
+			};
+			// entries [h, hend) of the list, hend - h a multiple of Q
+			auto groups = [&](int h, int hend)
+			{
+				for (; h < hend; h += Q)
+				{
+					uint2 en[Q];
+#pragma unroll
+					for (int q = 0; q < Q; q += 2)
 					{
-						const int o = out_col<E>(v, lane);
-						const bool in = a.o_begin + o < G.ld;
-						load_row<E>(row0, o, in, s0[v]);
-						load_row<E>(row1, o, in && two, s1[v]);
+						if (q + 1 < Q)
+						{
+							const uint4 t = *reinterpret_cast<const uint4*>(fl + h + q);
+							en[q] = make_uint2(t.x, t.y);
+							en[q + 1] = make_uint2(t.z, t.w);
+						}
+						else en[q] = fl[h + q];
+					}
+					float sv[Q][V][E];
+#pragma unroll
+					for (int q = 0; q < Q; q++)
+					{
+						const float* row = s32l + (size_t)en[q].x * ld;
+#pragma unroll
+						for (int v = 0; v < V; v++) load_row<E>(row, v * 32 * E, lcol + v * 32 * E < G.ld, sv[q][v]);
 					}
 #pragma unroll
 					for (int v = 0; v < V; v++)
 #pragma unroll
 						for (int e = 0; e < E; e++)
-						{
-							acc[v][e] = fma(w0, s0[v][e], acc[v][e]);
-							if (two) acc[v][e] = fma(w1, s1[v][e], acc[v][e]);
-						}
+#pragma unroll
+							for (int q = 0; q < Q; q++)
+								part[v][e] = __fmaf_rn(__uint_as_float(en[q].y), sv[q][v][e], part[v][e]);
+					since += Q;
+					if (since >= FLUSH) { flush(); since = 0; }
 				}
-				// Q rows in flight; a window's fine terms are summed in FP32 and
-				// the sum is added to the FP64 running sum once per window
-				if (fm)
+			};
+			traverse<true>(G, xs, lane, lo_n, hi_n, [&](unsigned mask, int n0, double w, const uint4& rec, float rm)
+			{
+				const bool mine = (mask >> lane) & 1u;
+				const float wf = __double2float_rn(w);
+				const float bound = fabsf(wf) * rm;
+				const bool big = mine && (rec.z & NODE_COARSE) && bound >= G.big_below;
+				const bool fine = mine && !big && bound >= G.skip_below;
+				unsigned cm = __ballot_sync(FULL, big);
+				const unsigned fm = __ballot_sync(FULL, fine);
+				if (fine) fl[cnt + __popc(fm & ((1u << lane) - 1u))] = make_uint2((uint32_t)(n0 + lane), __float_as_uint(wf));
+				cnt += __popc(fm);
+				if (cm)
 				{
-					float part[V][E];
-#pragma unroll
-					for (int v = 0; v < V; v++)
-#pragma unroll
-						for (int e = 0; e < E; e++) part[v][e] = 0.f;
-					while (fm)
+					const uint32_t ci = big ? __ldg(G.coarse_index + n0 + lane) : 0u;
+					// big terms two at a time (two FP64 rows in flight)
+					while (cm)
 					{
-						float wf[Q];
-						const float* row[Q];
-#pragma unroll
-						for (int q = 0; q < Q; q++)
-						{
-							const bool have = fm != 0u;
-							const int k = have ? __ffs(fm) - 1 : 0;
-							if (have) fm &= fm - 1;
-							wf[q] = have ? __double2float_rn(__shfl_sync(FULL, w, k)) : 0.f;
-							row[q] = G.s32 + (size_t)(n0 + k) * G.ld + a.o_begin;
-						}
-						float sv[Q][V][E];
+						const int k0 = __ffs(cm) - 1;
+						cm &= cm - 1;
+						const bool two = cm != 0u;
+						const int k1 = two ? __ffs(cm) - 1 : k0;
+						if (two) cm &= cm - 1;
+						const double w0 = __shfl_sync(FULL, w, k0);
+						const double w1 = __shfl_sync(FULL, w, k1);
+						const double* row0 = s64l + (size_t)__shfl_sync(FULL, ci, k0) * ld;
+						const double* row1 = s64l + (size_t)__shfl_sync(FULL, ci, k1) * ld;
+						double s0[V][E], s1[V][E];
 #pragma unroll
 						for (int v = 0; v < V; v++)
 						{
-							const int o = out_col<E>(v, lane);
-							const bool in = a.o_begin + o < G.ld;
-#pragma unroll
-							for (int q = 0; q < Q; q++) load_row<E>(row[q], o, in, sv[q][v]);
+							const bool in = lcol + v * 32 * E < G.ld;
+							load_row<E>(row0, v * 32 * E, in, s0[v]);
+							load_row<E>(row1, v * 32 * E, in && two, s1[v]);
 						}
 #pragma unroll
 						for (int v = 0; v < V; v++)
 #pragma unroll
 							for (int e = 0; e < E; e++)
-#pragma unroll
-								for (int q = 0; q < Q; q++) part[v][e] = __fmaf_rn(wf[q], sv[q][v][e], part[v][e]);
+							{
+								acc[v][e] = fma(w0, s0[v][e], acc[v][e]);
+								if (two) acc[v][e] = fma(w1, s1[v][e], acc[v][e]);
+							}
 					}
-#pragma unroll
-					for (int v = 0; v < V; v++)
-#pragma unroll
-						for (int e = 0; e < E; e++) acc[v][e] = __dadd_rn(acc[v][e], (double)part[v][e]);
+				}
+				if (cnt >= 32)
+				{
+					// all whole groups; the remainder (< Q entries) moves to the front
+					__syncwarp();
+					const int whole = cnt - cnt % Q;
+					groups(0, whole);
+					const int rem = cnt - whole;
+					uint2 t = make_uint2(0u, 0u);
+					if (lane < rem) t = fl[whole + lane];
+					__syncwarp();
+					if (lane < rem) fl[lane] = t;
+					__syncwarp();
+					cnt = rem;
 				}
 			}, wpath);
+			if (cnt)
+			{
+				// pad to whole groups with weight-0 copies of the first entry
+				const int padded = (cnt + Q - 1) / Q * Q;
+				__syncwarp();
+				const uint32_t r0 = fl[0].x;
+				if (lane >= cnt && lane < padded) fl[lane] = make_uint2(r0, 0u);
+				__syncwarp();
+				groups(0, padded);
+			}
+			flush();
 		}
 #pragma unroll
 		for (int v = 0; v < V; v++)
@@ -737,16 +830,27 @@ std::atomic<int> g_chunk_override{[]() { const char* e = getenv("SGI_CHUNK_ROWS"
 
 int chunk_rows_env() { return g_chunk_override.load(); }
 
+// FP32C variant of the direct entry points (plans time their own).
+constexpr int DEFAULT_VARIANT = 0;
+std::atomic<int> g_variant{DEFAULT_VARIANT};
+
 // Forward kernel for a pass of `cols` outputs with row stride ld.  variant
 // (FP32C only) trades fine rows in flight per warp against warps per SM:
 // 0 = two rows, registers as needed; 1 = four rows, at least 3 blocks per SM;
 // 2 = two rows, at least 4 blocks per SM.  Plans time all three.
+// FP32C kernel variants (rows in flight per warp against warps per SM):
+// 0 = groups of four rows, at least 3 blocks per SM; 1 = two rows, 4 blocks;
+// 2 = eight rows, 2 blocks.  Plans time all of them.
 constexpr int NVARIANTS = 3;
 template <int V, int E>
 void (*f32c_variant(int variant))(FwdArgs)
 {
-	return variant == 1 ? fwd_f32c_kernel<V, E, 4, 3> : variant == 2 ? fwd_f32c_kernel<V, E, 2, 4>
-	                                                                 : fwd_f32c_kernel<V, E, 2, 1>;
+	switch (variant)
+	{
+	case 1: return fwd_f32c_kernel<V, E, 2, 4>;
+	case 2: return fwd_f32c_kernel<V, E, 8, 2>;
+	default: return fwd_f32c_kernel<V, E, 4, 3>;
+	}
 }
 
 void (*select_fwd(int precision, int ld, int cols, int variant = 0))(FwdArgs)
@@ -754,8 +858,17 @@ void (*select_fwd(int precision, int ld, int cols, int variant = 0))(FwdArgs)
 	const bool f64 = precision == SGI_FP64;
 	if (ld <= 32) return f64 ? fwd_f64_kernel<1, 1> : f32c_variant<1, 1>(variant);
 	if (cols <= 64) return f64 ? fwd_f64_kernel<1, 2> : f32c_variant<1, 2>(variant);
-	if (cols <= 128) return f64 ? fwd_f64_kernel<2, 2> : f32c_variant<2, 2>(variant);
-	return f64 ? fwd_f64_kernel<4, 2> : f32c_variant<4, 2>(variant);
+	// FP32C reads four consecutive outputs per lane (16-byte loads) when rows
+	// are a multiple of 128 wide
+	const bool e4 = !f64 && ld % 128 == 0;
+	if (cols <= 128) return f64 ? fwd_f64_kernel<2, 2> : e4 ? f32c_variant<1, 4>(variant) : f32c_variant<2, 2>(variant);
+	return f64 ? fwd_f64_kernel<4, 2> : e4 ? f32c_variant<2, 4>(variant) : f32c_variant<4, 2>(variant);
+}
+
+// Dynamic shared memory of a forward launch.
+size_t fwd_smem(int precision, int dim)
+{
+	return (size_t)WARPS * (precision == SGI_FP32C ? list_stride(dim) : dim) * sizeof(double);
 }
 
 int pick_R(int cols)
@@ -805,7 +918,7 @@ int chunk_rows(const DeviceWork* W, const sgi_grid* g0, int precision, long long
 {
 	const int env = chunk_rows_env();
 	if (env >= 0) return env >= maxnno ? 0 : env;
-	// rows filling one L2 (FP64) or two (FP32C, whose coarse rows and
+	// rows filling one L2 (FP64) or two (FP32C, whose big terms and
 	// dropped terms leave part of each chunk unread): the autotuner's choice
 	// on the d=59, 1M-node, TotalDof=256 workload
 	const long long row = (long long)g0->ld * (precision == SGI_FP64 ? 8 : 4);
@@ -836,7 +949,9 @@ GridDesc desc_of(const sgi_grid* g, long long pt_begin, int precision = SGI_FP64
 	d.rec = g->rec; d.comps = g->comps;
 	d.rowmax = precision == SGI_FP32C ? g->rowmax : nullptr;
 	d.aux = g->aux;
-	d.skip_below = precision == SGI_FP32C ? g->skip_below : 0.f; d.s64 = g->s64; d.s32 = g->s32; d.s64c = g->s64c;
+	d.skip_below = precision == SGI_FP32C ? g->skip_below : 0.f;
+	d.big_below = precision == SGI_FP32C ? (float)g->info.coarse_threshold : 0.f;
+	d.s64 = g->s64; d.s32 = g->s32; d.s64c = g->s64c;
 	d.coarse_index = g->coarse_index; d.parent = g->parent; d.pt_begin = pt_begin; d.nno = g->nno; d.ld = g->ld;
 	return d;
 }
@@ -957,6 +1072,13 @@ extern "C" int sgi_set_chunk_rows(int rows)
 	return prev;
 }
 
+extern "C" int sgi_set_fp32c_variant(int variant)
+{
+	clear_error();
+	if (variant >= NVARIANTS) return fail(SGI_E_INVALID, "FP32C variant %d out of range (0..%d)", variant, NVARIANTS - 1);
+	return g_variant.exchange(variant < 0 ? DEFAULT_VARIANT : variant);
+}
+
 extern "C" int sgi_last_launch(sgi_launch_stats* s)
 {
 	if (!s) return fail(SGI_E_INVALID, "null argument");
@@ -988,8 +1110,9 @@ int check_set(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets)
 // from the device workspace's ring.
 int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets, const double* x,
 	double* out, int precision, cudaStream_t stream, int chunk = -1, unsigned long long* counters = nullptr,
-	int* nlaunch = nullptr, int variant = 2)
+	int* nlaunch = nullptr, int variant = -1)
 {
+	if (variant < 0) variant = g_variant.load();
 	const sgi_grid* g0 = grids[0];
 	DeviceWork* W = nullptr;
 	int rc = device_work(g0->device, &W);
@@ -997,8 +1120,9 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 	if (precision == SGI_FP64) { for (int k = 0; k < ngrids; k++) if (!grids[k]->s64) return fail(SGI_E_INVALID, "grid %d has no FP64 surplus", k); }
 	else if (precision == SGI_FP32C) { for (int k = 0; k < ngrids; k++) if (!grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k); }
 	else return fail(SGI_E_INVALID, "unknown precision %d", precision);
-	// per warp: the point's coordinates, and for FP32C the weight stack
-	const size_t smem = (size_t)WARPS * (g0->dim + (precision == SGI_FP32C ? WPATH : 0)) * sizeof(double);
+	// per warp: the point's coordinates, and for FP32C the weight stack (and
+	// the list form's term list)
+	const size_t smem = fwd_smem(precision, g0->dim);
 	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	g_stats = sgi_launch_stats{};
 	int launches = 0;
@@ -1331,7 +1455,8 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		if (precision == SGI_FP32C && !grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k);
 	}
 	const sgi_grid* g0 = grids[0];
-	const size_t smem = (size_t)WARPS * (g0->dim + (precision == SGI_FP32C ? WPATH : 0)) * sizeof(double);
+	const int variant = 0;
+	const size_t smem = fwd_smem(precision, g0->dim);
 	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	// count the launches first: reject before launching anything
 	const int passes = (g0->TD + PASS - 1) / PASS;
@@ -1367,7 +1492,7 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 			a.o_begin = ob;
 			a.counter = counters + slot++;
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS));
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, sms, &blocks);

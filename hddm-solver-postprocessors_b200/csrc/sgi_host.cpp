@@ -737,7 +737,7 @@ double coarse_threshold_for(const HostGrid& g)
 	static const double rel = []()
 	{
 		const char* e = getenv("SGI_COARSE_REL");
-		return e ? atof(e) : 0x1.0p-12;
+		return e ? atof(e) : 0x1.0p-16;
 	}();
 	return m * rel;
 }

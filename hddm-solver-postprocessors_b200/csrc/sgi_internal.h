@@ -37,7 +37,7 @@ enum NodeFlags : uint32_t
 	NODE_ALWAYS = 1u << 8,  // no components: weight 1 everywhere
 	NODE_DEAD   = 1u << 9,  // a component with i = 0, j != 0: weight 0 everywhere
 	NODE_MULTI  = 1u << 10, // activity needs all components checked
-	NODE_COARSE = 1u << 11, // FP32 form keeps a lo row for this node
+	NODE_COARSE = 1u << 11, // FP32C keeps an FP64 copy of this node's row
 };
 
 struct DeviceLayout
@@ -57,7 +57,9 @@ struct DeviceLayout
 // Builds the containment tree over the grid's node order and the records.
 int build_layout(const HostGrid& g, DeviceLayout& L);
 
-// Rows whose largest |surplus| is at least this keep an FP32 lo row.
+// Rows whose largest |surplus| is at least this keep an FP64 copy for the
+// FP32C form's big terms (2^-16 of the grid's largest |surplus|, or
+// SGI_COARSE_REL times it).
 double coarse_threshold_for(const HostGrid& g);
 
 } // namespace sgi

@@ -74,6 +74,7 @@ def _load():
         "sgi_active_count": (I, [P, LL, P, P, P]),
         "sgi_last_launch": (I, [ctypes.POINTER(LaunchStats)]),
         "sgi_set_chunk_rows": (I, [I]),
+        "sgi_set_fp32c_variant": (I, [I]),
         "sgi_plan_create": (I, [I, P, P, P, P, I, I, P, ctypes.POINTER(P)]),
         "sgi_plan_launch": (I, [P, P]),
         "sgi_plan_info": (I, [P, _c_int_p, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_float)]),
@@ -346,6 +347,15 @@ class Plan:
 def set_chunk_rows(rows):
     """-1 automatic, 0 never chunk, n > 0 chunks of n nodes; returns the previous setting."""
     return lib.sgi_set_chunk_rows(rows)
+
+
+def set_fp32c_variant(variant):
+    """FP32C kernel variant of interpolate/interpolate_host (-1: default);
+    returns the previous one."""
+    rc = lib.sgi_set_fp32c_variant(variant)
+    if rc < 0:
+        _check(rc)
+    return rc
 
 
 def last_launch():

@@ -113,7 +113,7 @@ int sgi_host_grid_tree(sgi_host_grid_t g, int* skip, int* parent);
 typedef struct sgi_grid* sgi_grid_t;
 
 /* Build flags */
-#define SGI_BUILD_FP32    0x1u   /* also keep the FP32 hi (+ lo for coarse rows) surplus */
+#define SGI_BUILD_FP32    0x1u   /* also keep the FP32 surplus (+ FP64 copies of coarse rows) */
 #define SGI_BUILD_NO_FP64 0x2u   /* drop the FP64 surplus (FP32 forms only)              */
 
 typedef struct sgi_grid_info
@@ -124,7 +124,7 @@ typedef struct sgi_grid_info
 	int tree_depth;       /* depth of the containment tree                       */
 	int tree_roots;       /* nodes without a containing ancestor                  */
 	int multi_delta;      /* nodes that differ from their tree parent in >1 dim   */
-	int ncoarse;          /* rows kept as FP32 hi+lo                              */
+	int ncoarse;          /* rows with an FP64 copy for FP32C big terms           */
 	long long comps;      /* stored (dim, i, j) components                        */
 	long long device_bytes;
 	double coarse_threshold;
@@ -140,7 +140,7 @@ void sgi_grid_destroy(sgi_grid_t g);
 
 /* ---------------------------------------------------------- interpolate */
 #define SGI_FP64   0   /* plain FP64: node order and rounding of the gold kernel */
-#define SGI_FP32C  1   /* FP32 surplus products, hi/lo coarse rows, compensated sums, FP64 final */
+#define SGI_FP32C  1   /* FP32 products of small terms, FP64 big terms and sums, FP64 final */
 
 /* Batched forward over a set of grids sharing dim and TotalDof (a multistate
  * set or a single grid): grid g owns points [pt_offsets[g], pt_offsets[g+1]).
@@ -206,6 +206,15 @@ int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* o
  * chunked); 0: never chunk; > 0: chunks of `rows` nodes.  Returns the previous
  * setting.  No reference counterpart. */
 int sgi_set_chunk_rows(int rows);
+
+/* FP32C kernel variant used by sgi_interpolate and sgi_interpolate_host
+ * (plans pick their own by timing): 0 = four surplus rows in flight per warp,
+ * 1 = two rows and more warps per SM, 2 = eight rows and fewer warps.  The
+ * variants interleave the FP64 additions of big terms and of FP32 partial
+ * sums differently, so their results may differ in the last bits (all within
+ * the FP32C tolerance).  variant < 0 restores the default (0).  Returns the
+ * previous setting, or a negative error code.  No reference counterpart. */
+int sgi_set_fp32c_variant(int variant);
 
 /* Plans: one forward call recorded into a CUDA graph and replayed.
  * sgi_plan_create records every launch of sgi_interpolate(ngrids, grids,

@@ -223,10 +223,12 @@ def test_graph_plan_bit_exact_and_replayable(cuda, chunk_rows):
         if chunk_rows >= 0:
             assert plan.chunk_rows == chunk_rows
         prev = H.set_chunk_rows(plan.chunk_rows)
+        prev_v = H.set_fp32c_variant(plan.variant)
         try:
             direct = H.interpolate(grids, x, counts=counts, precision=precision).cpu().numpy()
         finally:
             H.set_chunk_rows(prev)
+            H.set_fp32c_variant(prev_v)
         for _ in range(3):
             out.fill_(float("nan"))
             plan.launch()
@@ -240,6 +242,28 @@ def test_graph_plan_bit_exact_and_replayable(cuda, chunk_rows):
                 assert np.array_equal(got[sub], ref), k
             else:
                 assert O.rel_error(got[sub], ref)[0] <= FP32C_TOL, k
+
+
+@pytest.mark.parametrize("variant", range(3))
+@pytest.mark.parametrize("td,rows", [(256, 0), (256, 1500), (128, 0), (300, 2000), (64, 0), (20, 0)])
+def test_fp32c_variants_within_tolerance(cuda, variant, td, rows):
+    """Every FP32C kernel variant (E = 1, 2 and 4 output layouts, one and two
+    output passes, chunked or not) stays within the FP32C tolerance of gold,
+    and the FP64 form stays bit-exact under the same settings."""
+    h = H.HostGrid.adaptive(59, 6000, td, seed=60 + td)
+    g = H.Grid(h, flags=H.BUILD_FP32)
+    X = H.gen_points(59, 700, kind=2, seed=61)
+    prev, prev_v = H.set_chunk_rows(rows), H.set_fp32c_variant(variant)
+    try:
+        out32 = _run(g, X, H.FP32C)
+        out64 = _run(g, X, H.FP64)
+    finally:
+        H.set_chunk_rows(prev)
+        H.set_fp32c_variant(prev_v)
+    ref = O.Gold(*h.arrays()).interpolate(X)
+    assert np.array_equal(out64, ref)
+    e = O.rel_error(out32, ref)
+    assert e[0] <= FP32C_TOL, (variant, td, rows, e)
 
 
 def test_wide_component_form_bit_exact(cuda):
