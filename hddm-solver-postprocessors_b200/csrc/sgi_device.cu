@@ -64,9 +64,16 @@ struct GridDesc
 	int ld;
 };
 
+// Nodes of a chunk boundary's ancestor chain kept per grid (depths 1..CHAIN).
+constexpr int CHAIN = 31;
+
 struct FwdArgs
 {
 	GridDesc g[MAXG];
+	// ancestor chain of the chunk start per grid: chain[k][d - 1] is the node
+	// at depth d whose subtree contains the chunk start, d = 1..chain_len[k]
+	uint32_t chain[MAXG][CHAIN];
+	int chain_len[MAXG];
 	const double* x;
 	double* out;
 	unsigned long long* counter;
@@ -156,9 +163,13 @@ constexpr int WPATH = 64;
 // warp OR reduction gives every lane whether an earlier failing node covers
 // it; the next window starts at the larger of n0+32 and the largest failing
 // skip (one warp max reduction).
-// A node whose tree parent lies before `a` ("chunk root") is checked on all its
-// components, since its ancestors are not walked; inside the range a node is
-// reached only when all its ancestors in the range are active.
+// Inside the range a node is reached only when all its ancestors in the range
+// are active.  A node whose tree parent lies before `a` ("chunk root") has its
+// parent in the chunk start's ancestor chain: bit d of pathmask tells whether
+// the chain node at depth d is active (bit 0 stands for the roots' parent),
+// and the chunk root is then decided by its delta hat like any other node.
+// Chunk roots whose parent is deeper than the chain's clen stored levels are
+// checked on all their components.
 // Without INCR every hit takes the full product (the FP64 form: gold's
 // multiplies in gold's order).
 // INCR (FP32C): a hit's weight is its tree parent's weight times its delta
@@ -171,7 +182,7 @@ constexpr int WPATH = 64;
 // deeper than the stack take the full product.
 template <bool INCR, class OnHits>
 __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, int a, int b,
-	OnHits&& on_hits, double* wpath = nullptr)
+	OnHits&& on_hits, double* wpath = nullptr, unsigned pathmask = 1u, int clen = 0)
 {
 	int n0 = a;
 	if (INCR)
@@ -190,7 +201,7 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 		rn = __ldg(G.rec + n0 + lane);
 		if (INCR || a > 0) pn = __ldg(G.parent + n0 + lane);
 		if (G.rowmax) mn = __ldg(G.rowmax + n0 + lane);
-		if (INCR) xn = __ldg(G.aux + n0 + lane);
+		if (INCR || a > 0) xn = __ldg(G.aux + n0 + lane);
 	}
 	while (n0 < b)
 	{
@@ -205,8 +216,11 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 		double factor = 1.0;
 		if (valid)
 		{
+			// depth of a chunk root's parent: ax.y - 1 (0 for tree roots)
+			const bool croot_full = chunk_root && (ax.y == 0u || (int)ax.y - 1 > clen);
 			if (r.z & NODE_DEAD) act = false;
-			else if ((r.z & NODE_MULTI) || chunk_root) { act = node_active(G, xs, r.y, ncomp); full = true; }
+			else if ((r.z & NODE_MULTI) || croot_full) { act = node_active(G, xs, r.y, ncomp); full = true; }
+			else if (chunk_root && !((pathmask >> (ax.y - 1u)) & 1u)) act = false;
 			else if (r.z & NODE_ALWAYS) act = true;
 			else
 			{
@@ -237,7 +251,7 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 			rn = __ldg(G.rec + nnext + lane);
 			if (INCR || a > 0) pn = __ldg(G.parent + nnext + lane);
 			if (G.rowmax) mn = __ldg(G.rowmax + nnext + lane);
-			if (INCR) xn = __ldg(G.aux + nnext + lane);
+			if (INCR || a > 0) xn = __ldg(G.aux + nnext + lane);
 		}
 		double w = 0.0;
 		if (!INCR) w = hit ? node_weight(G, xs, r.y, ncomp) : 0.0;
@@ -270,6 +284,35 @@ template <class OnHits>
 __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, int lane, OnHits&& on_hits)
 {
 	traverse<false>(G, xs, lane, 0, G.nno, on_hits);
+}
+
+// Activity (bit d of the result; bit 0 set) and, when wpath is given, weight
+// (wpath[d]; 0 when inactive) of the chunk start's ancestor chain for the
+// point in xs: lane d evaluates the chain node at depth d on all its
+// components.  A chunk root's parent is one of these nodes.  Every node
+// before the end of the shallowest inactive chain node's subtree is
+// inactive, so *start moves there.
+__device__ __forceinline__ unsigned chain_state(const FwdArgs& a, int gi, const GridDesc& G, const double* xs,
+	int lane, double* wpath, int* start)
+{
+	const int len = a.chain_len[gi];
+	if (len == 0) return 1u;
+	bool act = false;
+	double w = 0.0;
+	uint32_t skip = 0u;
+	if (lane >= 1 && lane <= len)
+	{
+		const uint4 r = __ldg(G.rec + a.chain[gi][lane - 1]);
+		skip = r.x;
+		act = node_active(G, xs, r.y, r.z & 0xffu);
+		if (wpath && act) w = node_weight(G, xs, r.y, r.z & 0xffu);
+	}
+	if (wpath && lane >= 1 && lane <= len) wpath[lane] = w;
+	const unsigned m = __ballot_sync(FULL, act) | 1u;
+	const unsigned inactive = ~m & ((2u << len) - 2u);   // depths 1..len
+	const uint32_t end = __shfl_sync(FULL, skip, inactive ? __ffs(inactive) - 1 : 0);
+	if (inactive) *start = max(*start, (int)end);
+	return m;
 }
 
 // Node range of this launch for grid G.
@@ -347,10 +390,19 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 		if (lane == 0) p = (long long)atomicAdd(a.counter, 1ull);
 		p = __shfl_sync(FULL, p, 0);
 		if (p >= a.npts) break;
-		const GridDesc& G = a.g[find_grid(a, p)];
+		const int gi = find_grid(a, p);
+		const GridDesc& G = a.g[gi];
 		int lo, hi;
 		chunk_of(a, G, &lo, &hi);
 		if (!first && lo >= hi) continue;   // this grid has no nodes in the chunk
+		const bool ok = load_point(a, p, xs, lane);
+		if (!ok && !first) continue;        // NaN already written by the first chunk
+		unsigned pathmask = 1u;
+		if (!first)
+		{
+			pathmask = chain_state(a, gi, G, xs, lane, nullptr, &lo);
+			if (lo >= hi) continue;         // no active node in the chunk: outputs unchanged
+		}
 		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
 		// the running sums continue from the previous chunk, so the adds keep
 		// the gold loop's order across chunks
@@ -363,8 +415,6 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 				const int o = out_col<E>(v, lane) + e;
 				acc[v][e] = (!first && a.o_begin + o < a.TD) ? __ldcs(dst + o) : 0.0;
 			}
-		const bool ok = load_point(a, p, xs, lane);
-		if (!ok && !first) continue;        // NaN already written by the first chunk
 		if (ok)
 		{
 			traverse<false>(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&, float)
@@ -400,7 +450,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 							if (two) acc[v][e] = __dadd_rn(acc[v][e], __dmul_rn(w1, s1[v][e]));
 						}
 				}
-			});
+			}, nullptr, pathmask, a.chain_len[gi]);
 		}
 #pragma unroll
 		for (int v = 0; v < V; v++)
@@ -453,10 +503,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 		if (lane == 0) p = (long long)atomicAdd(a.counter, 1ull);
 		p = __shfl_sync(FULL, p, 0);
 		if (p >= a.npts) break;
-		const GridDesc& G = a.g[find_grid(a, p)];
+		const int gi = find_grid(a, p);
+		const GridDesc& G = a.g[gi];
 		int lo_n, hi_n;
 		chunk_of(a, G, &lo_n, &hi_n);
 		if (!first && lo_n >= hi_n) continue;   // this grid has no nodes in the chunk
+		const bool ok = load_point(a, p, xs, lane);
+		if (!ok && !first) continue;            // NaN already written by the first chunk
+		unsigned pathmask = 1u;
+		if (!first)
+		{
+			pathmask = chain_state(a, gi, G, xs, lane, wpath, &lo_n);
+			if (lo_n >= hi_n) continue;         // no active node in the chunk: outputs unchanged
+		}
 		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
 		double acc[V][E];
 #pragma unroll
@@ -467,8 +526,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 				const int o = out_col<E>(v, lane) + e;
 				acc[v][e] = (!first && a.o_begin + o < a.TD) ? __ldcs(dst + o) : 0.0;
 			}
-		const bool ok = load_point(a, p, xs, lane);
-		if (!ok && !first) continue;            // NaN already written by the first chunk
 		if (ok)
 		{
 			const int lcol = a.o_begin + out_col<E>(0, lane);
@@ -582,7 +639,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 					__syncwarp();
 					cnt = rem;
 				}
-			}, wpath);
+			}, wpath, pathmask, a.chain_len[gi]);
 			if (cnt)
 			{
 				// pad to whole groups with weight-0 copies of the first entry
@@ -909,6 +966,10 @@ struct sgi_grid
 	double* s64c = nullptr;
 	uint32_t* coarse_index = nullptr;
 	int* parent = nullptr;
+	// host copy of the containment tree, for the ancestor chains of node
+	// chunk boundaries
+	std::vector<int> parent_h;
+	std::vector<uint32_t> skip_h, depth_h;
 	sgi_grid_info info{};
 };
 
@@ -1009,6 +1070,11 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 	if (!rc) rc = upload((void**)&d->comps, L.comps.data(), L.comps.size() * 4);
 	if (!rc) rc = upload((void**)&d->coarse_index, L.lo_index.data(), L.lo_index.size() * 4);
 	if (!rc) rc = upload((void**)&d->parent, L.parent.data(), L.parent.size() * 4);
+	if (!rc) rc = upload((void**)&d->aux, L.aux.data(), L.aux.size() * 4);
+	d->parent_h = L.parent;
+	d->skip_h.resize(g.nno);
+	d->depth_h.resize(g.nno);
+	for (int n = 0; n < g.nno; n++) { d->skip_h[n] = L.rec[4 * (size_t)n]; d->depth_h[n] = L.aux[2 * (size_t)n + 1]; }
 	if (!rc && !(flags & SGI_BUILD_NO_FP64))
 	{
 		std::vector<double> s(nrow * d->ld, 0.0);
@@ -1042,7 +1108,6 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 			smax = std::max(smax, m);
 		}
 		if (!rc) rc = upload((void**)&d->rowmax, rmax.data(), rmax.size() * 4);
-		if (!rc) rc = upload((void**)&d->aux, L.aux.data(), L.aux.size() * 4);
 		d->skip_below = (float)(ldexp(smax, -46));
 	}
 	if (rc) { free_grid(d); return rc; }
@@ -1105,6 +1170,32 @@ int check_set(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets)
 	return SGI_OK;
 }
 
+// Ancestor chain of a node-chunk start c0: the nodes p < c0 whose subtree
+// range [p, skip[p]) reaches past c0, stored by depth (out[d - 1] is the one
+// at depth d, d = 1..CHAIN); returns the number stored.  The tree parent of
+// every chunk root (a node at or after c0 whose parent precedes c0) is in
+// this chain: its range holds both the parent and the chunk root.  The chain
+// is the part of the ancestor path of the last live node before c0 that is
+// still open at c0; every ancestor of an open node is open, so the stored
+// depths run from 1 without gaps.
+int chain_at(const sgi_grid* g, int c0, uint32_t* out)
+{
+	if (c0 <= 0 || c0 >= g->nno) return 0;
+	int q = c0 - 1;
+	while (q >= 0 && g->depth_h[q] == 0) q--;   // dead nodes are outside the tree
+	uint32_t filled = 0;
+	for (; q >= 0; q = g->parent_h[q])
+		if (g->skip_h[q] > (uint32_t)c0)
+		{
+			const uint32_t d = g->depth_h[q];
+			if (d >= 1 && d <= (uint32_t)CHAIN) { out[d - 1] = (uint32_t)q; filled |= 1u << (d - 1); }
+		}
+	// depths 1..len, stopping at a gap (none in a tree; kept as a guard)
+	int len = 0;
+	while (len < CHAIN && ((filled >> len) & 1u)) len++;
+	return len;
+}
+
 // Launches of one forward call.  chunk < 0: the automatic chunk size; work
 // counters come from `counters` (one per launch, in order) when given, else
 // from the device workspace's ring.
@@ -1148,6 +1239,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 			a.o_begin = ob;
 			a.chunk_begin = c * clen;
 			a.chunk_len = clen;
+			for (int k = 0; k < ng; k++) a.chain_len[k] = chain_at(grids[gb + k], a.chunk_begin, a.chain[k]);
 			a.counter = counters ? counters + launches : W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
 			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant);

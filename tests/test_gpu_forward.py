@@ -162,6 +162,32 @@ def test_file_order_not_depth_first_still_exact(cuda):
     assert np.array_equal(_run(g, X), O.Gold(idx[perm], sur[perm]).interpolate(X))
 
 
+@pytest.mark.parametrize("rows", [1, 2, 3, 5, 17, 64])
+def test_chunk_boundaries_everywhere(cuda, rows):
+    """Tiny node chunks put a boundary inside every subtree: chunk roots are
+    decided from the boundary's ancestor chain.  Depth-first grids, a grid
+    in random order (many tree roots) and never-active nodes between live
+    ones; FP64 stays bit-exact, FP32C within tolerance."""
+    idx, sur = H.HostGrid.adaptive(8, 600, 16, seed=7).arrays()
+    dead_i = np.zeros((3, idx.shape[1]), np.int32)
+    dead_i[:, 8:] = 3                      # i = 0, j = 3 in every dimension: never active
+    cases = [(idx, sur)]
+    ins = np.insert(idx, [0, 1, 40, 41, 300], dead_i[[0, 1, 2, 0, 1]], axis=0)
+    cases.append((ins, np.insert(sur, [0, 1, 40, 41, 300], 0.5, axis=0)))
+    perm = np.random.default_rng(2).permutation(len(idx))
+    cases.append((idx[perm], sur[perm]))
+    X = H.gen_points(8, 300, kind=2, seed=9)
+    prev = H.set_chunk_rows(rows)
+    try:
+        for ci, (i_, s_) in enumerate(cases):
+            g = H.Grid(H.HostGrid.from_dense(i_, s_), flags=H.BUILD_FP32)
+            ref = O.Gold(i_, s_).interpolate(X)
+            assert np.array_equal(_run(g, X), ref), ci
+            assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL, ci
+    finally:
+        H.set_chunk_rows(prev)
+
+
 def test_active_count_matches_oracle(cuda):
     import torch
     hg = H.HostGrid.adaptive(59, 20000, 4, seed=3)
