@@ -443,7 +443,7 @@ def run_chunksweep(args):
     x = torch.from_numpy(X).to(dev)
     out = torch.empty((X.shape[0], TD), dtype=torch.float64, device=dev)
     s = torch.cuda.current_stream(dev)
-    rows_list = [0, 32768, 49152, 65536, 98304, 131072, 196608, 262144]
+    rows_list = [0, 16384, 32768, 49152, 65536, 98304, 131072, 196608, 262144]
     res = {}
     for prec, name in ((H.FP32C, "fp32c"), (H.FP64, "fp64")):
         for rows in rows_list:

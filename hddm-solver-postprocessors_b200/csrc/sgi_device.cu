@@ -288,8 +288,13 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 
 // Activity (bit d of the result; bit 0 set) and, when wpath is given, weight
 // (wpath[d]; 0 when inactive) of the chunk start's ancestor chain for the
-// point in xs: lane d evaluates the chain node at depth d on all its
-// components.  A chunk root's parent is one of these nodes.  Every node
+// point in xs.  Lane d takes the chain node at depth d, whose parent is the
+// node at depth d - 1: as in the walk, it is active when its parent is and
+// its delta hat is positive, and its weight is the parent's times the delta
+// hat over the parent's hat in that dimension (a prefix AND over a ballot and
+// a segmented prefix product over the lanes; nodes differing from their
+// parent in several dimensions are evaluated on all components and start a
+// new segment).  A chunk root's parent is one of these nodes.  Every node
 // before the end of the shallowest inactive chain node's subtree is
 // inactive, so *start moves there.
 __device__ __forceinline__ unsigned chain_state(const FwdArgs& a, int gi, const GridDesc& G, const double* xs,
@@ -297,18 +302,50 @@ __device__ __forceinline__ unsigned chain_state(const FwdArgs& a, int gi, const 
 {
 	const int len = a.chain_len[gi];
 	if (len == 0) return 1u;
-	bool act = false;
-	double w = 0.0;
+	const bool mine = lane >= 1 && lane <= len;
+	bool local = true, multi = false;
+	double f = 1.0;
 	uint32_t skip = 0u;
-	if (lane >= 1 && lane <= len)
+	if (mine)
 	{
-		const uint4 r = __ldg(G.rec + a.chain[gi][lane - 1]);
+		const uint32_t node = a.chain[gi][lane - 1];
+		const uint4 r = __ldg(G.rec + node);
 		skip = r.x;
-		act = node_active(G, xs, r.y, r.z & 0xffu);
-		if (wpath && act) w = node_weight(G, xs, r.y, r.z & 0xffu);
+		if (r.z & NODE_MULTI)
+		{
+			multi = true;
+			local = node_active(G, xs, r.y, r.z & 0xffu);
+			if (wpath && local) f = node_weight(G, xs, r.y, r.z & 0xffu);
+		}
+		else if (!(r.z & NODE_ALWAYS))
+		{
+			const double xd = xs[r.z >> 16];
+			const double hd = hat(xd, r.w);
+			local = hd > 0.0;
+			if (wpath && local)
+			{
+				const uint32_t old = __ldg(G.aux + node).x;
+				f = old ? hd * rcp_weight(hat(xd, old)) : hd;
+			}
+		}
 	}
-	if (wpath && lane >= 1 && lane <= len) wpath[lane] = w;
-	const unsigned m = __ballot_sync(FULL, act) | 1u;
+	// active: every chain node shallower than the first local failure
+	const unsigned fails = __ballot_sync(FULL, mine && !local);
+	const unsigned upto = fails ? (1u << (__ffs(fails) - 1)) - 1u : FULL;
+	const unsigned m = (upto & ((2u << len) - 1u)) | 1u;
+	if (wpath)
+	{
+		double w = mine ? f : 1.0;
+		bool seg = multi || lane == 0;
+#pragma unroll
+		for (int off = 1; off < 32; off <<= 1)
+		{
+			const double wu = __shfl_up_sync(FULL, w, off);
+			const bool su = __shfl_up_sync(FULL, (int)seg, off);
+			if (lane >= off && !seg) { w *= wu; seg = su; }
+		}
+		if (mine) wpath[lane] = ((m >> lane) & 1u) ? w : 0.0;
+	}
 	const unsigned inactive = ~m & ((2u << len) - 2u);   // depths 1..len
 	const uint32_t end = __shfl_sync(FULL, skip, inactive ? __ffs(inactive) - 1 : 0);
 	if (inactive) *start = max(*start, (int)end);
