@@ -57,6 +57,10 @@ struct GridDesc
 	const int* parent;           // tree parent per node (-1 for roots)
 	const float* rowmax;         // largest |surplus| of each row (FP32C), or null
 	const uint2* aux;            // {parent's component in the delta dim, depth}: FP32C weights
+	const uint4* grp_a;          // descent child groups (FP32C): {L, R, d | kind << 16, parent's ij in d}
+	const uint2* grp_b;          //   {L's ij in d, R's}
+	const uint4* ninfo;          //   per node: {first group, group count, rowmax bits, FP64 copy row or NONE}
+	int depth;                   // containment-tree depth (bounds the descent stack)
 	float skip_below;            // FP32C drops fine terms with |w| * rowmax below this
 	float big_below;             // FP32C list form: terms with |w| * rowmax from this up are big
 	long long pt_begin;
@@ -74,6 +78,11 @@ struct FwdArgs
 	// at depth d whose subtree contains the chunk start, d = 1..chain_len[k]
 	uint32_t chain[MAXG][CHAIN];
 	int chain_len[MAXG];
+	// descent starts of this launch per grid: the child groups of the chain
+	// node at depth d that may hold nodes of the chunk (cseg[k][d - 1]), and
+	// the tree roots' groups that may (rseg[k]); {first, end}
+	uint2 cseg[MAXG][CHAIN];
+	uint2 rseg[MAXG];
 	const double* x;
 	double* out;
 	unsigned long long* counter;
@@ -83,6 +92,9 @@ struct FwdArgs
 	// every grid; chunk_len 0 means the whole grid
 	int chunk_begin, chunk_len;
 };
+
+// kernel parameters are limited to 32,764 bytes
+static_assert(sizeof(FwdArgs) <= 32764, "FwdArgs exceeds the kernel parameter limit");
 
 // Exact conversion of v < 2^32 to double in the FP64 pipe: the bit pattern
 // 0x43300000:v is 2^52 + v, and subtracting 2^52 is exact.
@@ -702,6 +714,302 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 	}
 }
 
+// ------------------------------------------------------------ descent walk
+//
+// FP32C form over the descent layout: instead of scanning node windows, the
+// warp keeps a stack (shared memory) of pending child-group ranges, each with
+// its parent's weight, and evaluates up to 32 groups per step, one per lane.
+// A pair group holds the left and right child of its parent in one
+// dimension (disjoint supports): the lane tests the left child's hat and, if
+// it is zero, the right one's, so at most one child per group is a hit and
+// nearly every lane evaluation finds one.  A hit's weight is its parent's
+// weight times its hat over the parent's hat in that dimension; a hit with
+// children in the launch's node range pushes its own group range.
+//
+// Stack bound: a step takes 32 groups while size + 32 + depth <= SCAP (depth
+// = the tree's depth), else one group from the top range.  A 32-group step
+// pushes at most 32 ranges, so it leaves at most SCAP - depth.  Single-group
+// steps push, above the ranges present when they began, a chain of ranges of
+// increasing tree depth (each one the children of a node taken from the range
+// below it): at most depth of them.  The starts are at most 32 ranges (the
+// roots' and one per chain node), so the size stays within SCAP whenever
+// depth <= SCAP - 32.  The host selects this kernel only then, and for
+// chunked launches only when every chain is complete (depth <= CHAIN + 1).
+constexpr int SCAP = 128;
+
+// Shared memory per warp of the descent form, in doubles: the stack (SCAP
+// 16-byte entries), the fine-term list, the chain weights and the point.
+__host__ __device__ __forceinline__ int desc_stride(int dim) { return 2 * SCAP + FCAP + 32 + ((dim + 1) & ~1); }
+
+__device__ __forceinline__ uint4 pack_seg(uint32_t b, uint32_t e, double w)
+{
+	return make_uint4(b, e, (uint32_t)__double2loint(w), (uint32_t)__double2hiint(w));
+}
+
+template <int V, int E, int Q, int MINB, bool FULLROW>
+__global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_constant__ FwdArgs a)
+{
+	static_assert(FLUSH % Q == 0 || Q % FLUSH == 0, "groups of Q must tile the flush interval");
+	static_assert(32 % Q == 0, "groups of Q must tile a step's hits");
+	extern __shared__ double smem[];
+	const int lane = threadIdx.x & 31;
+	double* wbase = smem + (threadIdx.x >> 5) * desc_stride(a.dim);
+	uint4* stk = reinterpret_cast<uint4*>(wbase);
+	uint2* fl = reinterpret_cast<uint2*>(wbase + 2 * SCAP);
+	double* wchain = wbase + 2 * SCAP + FCAP;
+	double* xs = wchain + 32;
+	const bool first = a.chunk_begin == 0;
+	for (;;)
+	{
+		long long p = 0;
+		if (lane == 0) p = (long long)atomicAdd(a.counter, 1ull);
+		p = __shfl_sync(FULL, p, 0);
+		if (p >= a.npts) break;
+		const int gi = find_grid(a, p);
+		const GridDesc& G = a.g[gi];
+		int lo_n, hi_n;
+		chunk_of(a, G, &lo_n, &hi_n);
+		if (!first && lo_n >= hi_n) continue;   // this grid has no nodes in the chunk
+		const bool ok = load_point(a, p, xs, lane);
+		if (!ok && !first) continue;            // NaN already written by the first chunk
+		// starts: lane 0 the roots' groups, lane d the groups of the active
+		// chain node at depth d (after the first chunk)
+		int size = 0;
+		if (ok)
+		{
+			unsigned pathmask = 1u;
+			const int len = first ? 0 : a.chain_len[gi];
+			if (len)
+			{
+				int unused = lo_n;
+				pathmask = chain_state(a, gi, G, xs, lane, wchain, &unused);
+			}
+			uint2 seg = make_uint2(0u, 0u);
+			double ws = 1.0;
+			if (lane == 0) seg = a.rseg[gi];
+			else if (lane <= len && ((pathmask >> lane) & 1u)) { seg = a.cseg[gi][lane - 1]; ws = wchain[lane]; }
+			const bool push = seg.y > seg.x;
+			const unsigned pm = __ballot_sync(FULL, push);
+			if (push) stk[__popc(pm & ((1u << lane) - 1u))] = pack_seg(seg.x, seg.y, ws);
+			size = __popc(pm);
+			__syncwarp();
+			if (!first && !size) continue;     // no active start in the chunk: outputs unchanged
+		}
+		double* dst = a.out + (size_t)p * a.TD + a.o_begin;
+		double acc[V][E];
+#pragma unroll
+		for (int v = 0; v < V; v++)
+#pragma unroll
+			for (int e = 0; e < E; e++)
+			{
+				const int o = out_col<E>(v, lane) + e;
+				acc[v][e] = (!first && (FULLROW || a.o_begin + o < a.TD)) ? __ldcs(dst + o) : 0.0;
+			}
+		if (size)
+		{
+			const int lcol = a.o_begin + out_col<E>(0, lane);
+			const float* s32l = G.s32 + lcol;
+			const double* s64l = G.s64c + lcol;
+			const uint32_t ld = (uint32_t)G.ld;
+			const float skip_below = G.skip_below, big_below = G.big_below;
+			const int bmax = SCAP - 32 - G.depth;   // 32-group steps while size <= bmax
+			float part[V][E];
+#pragma unroll
+			for (int v = 0; v < V; v++)
+#pragma unroll
+				for (int e = 0; e < E; e++) part[v][e] = 0.f;
+			int cnt = 0, since = 0;
+			auto flush = [&]()
+			{
+#pragma unroll
+				for (int v = 0; v < V; v++)
+#pragma unroll
+					for (int e = 0; e < E; e++) { acc[v][e] = __dadd_rn(acc[v][e], (double)part[v][e]); part[v][e] = 0.f; }
+			};
+			// list entries [h, hend), hend - h a multiple of Q
+			auto groups = [&](int h, int hend)
+			{
+				for (; h < hend; h += Q)
+				{
+					uint2 en[Q];
+#pragma unroll
+					for (int q = 0; q < Q; q += 2)
+					{
+						if (q + 1 < Q)
+						{
+							const uint4 t = *reinterpret_cast<const uint4*>(fl + h + q);
+							en[q] = make_uint2(t.x, t.y);
+							en[q + 1] = make_uint2(t.z, t.w);
+						}
+						else en[q] = fl[h + q];
+					}
+					float sv[Q][V][E];
+#pragma unroll
+					for (int q = 0; q < Q; q++)
+					{
+						const float* row = s32l + (size_t)en[q].x * ld;
+#pragma unroll
+						for (int v = 0; v < V; v++)
+							load_row<E>(row, v * 32 * E, FULLROW || lcol + v * 32 * E < (int)ld, sv[q][v]);
+					}
+#pragma unroll
+					for (int v = 0; v < V; v++)
+#pragma unroll
+						for (int e = 0; e < E; e++)
+#pragma unroll
+							for (int q = 0; q < Q; q++)
+								part[v][e] = __fmaf_rn(__uint_as_float(en[q].y), sv[q][v][e], part[v][e]);
+					since += Q;
+					if (since >= FLUSH) { flush(); since = 0; }
+				}
+			};
+			while (size > 0)
+			{
+				const int B = size <= bmax ? 32 : 1;
+				// lane k looks at stack entry size - 1 - k (lane 0: the top)
+				uint4 e = make_uint4(0u, 0u, 0u, 0u);
+				if (lane < size) e = stk[size - 1 - lane];
+				const uint32_t cntk = e.y - e.x;
+				uint32_t incl = cntk;
+#pragma unroll
+				for (int off = 1; off < 32; off <<= 1)
+				{
+					const uint32_t t = __shfl_up_sync(FULL, incl, off);
+					if (lane >= off) incl += t;
+				}
+				const uint32_t take = min((uint32_t)B, __shfl_sync(FULL, incl, 31));
+				const uint32_t start = incl - cntk;
+				// ranges taken whole leave the stack; the one taken in part
+				// (the new top) moves its first group
+				const unsigned whole = __ballot_sync(FULL, lane < size && incl <= take);
+				if (lane < size && start < take && incl > take) stk[size - 1 - lane].x = e.x + (take - start);
+				const unsigned starts = __reduce_or_sync(FULL, (lane < size && start < take) ? (1u << start) : 0u);
+				const int k = max(__popc(starts & ((2u << lane) - 1u)) - 1, 0);   // this lane's range
+				const uint32_t kb = __shfl_sync(FULL, e.x, k);
+				const uint32_t ks = __shfl_sync(FULL, start, k);
+				const double wp = __hiloint2double((int)__shfl_sync(FULL, e.w, k), (int)__shfl_sync(FULL, e.z, k));
+				size -= __popc(whole);
+				// evaluate group kb + lane - ks
+				uint32_t c = DESC_NONE;
+				double w = 0.0;
+				if ((uint32_t)lane < take)
+				{
+					const uint32_t gidx = kb + (uint32_t)lane - ks;
+					const uint4 ga = __ldg(G.grp_a + gidx);
+					const uint32_t kind = (ga.z >> 16) & 3u;
+					if (kind == DESC_SIMPLE)
+					{
+						const uint2 gb = __ldg(G.grp_b + gidx);
+						const double xd = xs[ga.z & 0xffffu];
+						double h = hat(xd, gb.x);
+						if (h > 0.0) c = ga.x;
+						else if (ga.y != DESC_NONE)
+						{
+							h = hat(xd, gb.y);
+							if (h > 0.0) c = ga.y;
+						}
+						if (c != DESC_NONE) w = ga.w ? wp * h * rcp_weight(hat(xd, ga.w)) : wp * h;
+					}
+					else if (kind == DESC_MULTI)
+					{
+						const uint4 r = __ldg(G.rec + ga.x);
+						if (node_active(G, xs, r.y, r.z & 0xffu)) { c = ga.x; w = node_weight(G, xs, r.y, r.z & 0xffu); }
+					}
+					else { c = ga.x; w = wp; }
+					if (c != DESC_NONE && ((int)c < lo_n || (int)c >= hi_n)) c = DESC_NONE;
+				}
+				const bool hit = c != DESC_NONE;
+				uint4 ni = make_uint4(0u, 0u, 0u, DESC_NONE);
+				if (hit) ni = __ldg(G.ninfo + c);
+				// hits with children in the range push their groups
+				const bool pushme = hit && ni.y && (int)c + 1 < hi_n;
+				const unsigned pm = __ballot_sync(FULL, pushme);
+				// the stack bound keeps size + pushes within SCAP; the test only
+				// stops a write past the stack
+				const int slot = size + __popc(pm & ((1u << lane) - 1u));
+				if (pushme && slot < SCAP) stk[slot] = pack_seg(ni.x, ni.x + ni.y, w);
+				size = min(size + __popc(pm), SCAP);
+				__syncwarp();
+				const unsigned mask = __ballot_sync(FULL, hit);
+				if (!mask) continue;
+				// big terms (rows with an FP64 copy, |w| * rowmax at or above the
+				// threshold) now; fine terms to the list; negligible ones dropped
+				const float wf = __double2float_rn(w);
+				const float bound = fabsf(wf) * __uint_as_float(ni.z);
+				const bool big = hit && ni.w != DESC_NONE && bound >= big_below;
+				const bool fine = hit && !big && bound >= skip_below;
+				unsigned cm = __ballot_sync(FULL, big);
+				const unsigned fm = __ballot_sync(FULL, fine);
+				if (fine) fl[cnt + __popc(fm & ((1u << lane) - 1u))] = make_uint2(c, __float_as_uint(wf));
+				cnt += __popc(fm);
+				while (cm)
+				{
+					const int k0 = __ffs(cm) - 1;
+					cm &= cm - 1;
+					const bool two = cm != 0u;
+					const int k1 = two ? __ffs(cm) - 1 : k0;
+					if (two) cm &= cm - 1;
+					const double w0 = __shfl_sync(FULL, w, k0);
+					const double w1 = __shfl_sync(FULL, w, k1);
+					const double* row0 = s64l + (size_t)__shfl_sync(FULL, ni.w, k0) * ld;
+					const double* row1 = s64l + (size_t)__shfl_sync(FULL, ni.w, k1) * ld;
+					double s0[V][E], s1[V][E];
+#pragma unroll
+					for (int v = 0; v < V; v++)
+					{
+						const bool in = FULLROW || lcol + v * 32 * E < (int)ld;
+						load_row<E>(row0, v * 32 * E, in, s0[v]);
+						load_row<E>(row1, v * 32 * E, in && two, s1[v]);
+					}
+#pragma unroll
+					for (int v = 0; v < V; v++)
+#pragma unroll
+						for (int e2 = 0; e2 < E; e2++)
+						{
+							acc[v][e2] = fma(w0, s0[v][e2], acc[v][e2]);
+							if (two) acc[v][e2] = fma(w1, s1[v][e2], acc[v][e2]);
+						}
+				}
+				if (cnt >= 32)
+				{
+					// all whole groups; the remainder (< Q entries) moves to the front
+					__syncwarp();
+					const int wholeq = cnt - cnt % Q;
+					groups(0, wholeq);
+					const int rem = cnt - wholeq;
+					uint2 t = make_uint2(0u, 0u);
+					if (lane < rem) t = fl[wholeq + lane];
+					__syncwarp();
+					if (lane < rem) fl[lane] = t;
+					__syncwarp();
+					cnt = rem;
+				}
+			}
+			if (cnt)
+			{
+				// pad to whole groups with weight-0 copies of the first entry
+				const int padded = (cnt + Q - 1) / Q * Q;
+				__syncwarp();
+				const uint32_t r0 = fl[0].x;
+				if (lane >= cnt && lane < padded) fl[lane] = make_uint2(r0, 0u);
+				__syncwarp();
+				groups(0, padded);
+			}
+			flush();
+		}
+#pragma unroll
+		for (int v = 0; v < V; v++)
+#pragma unroll
+			for (int e = 0; e < E; e++)
+			{
+				const int o = out_col<E>(v, lane) + e;
+				if (FULLROW || a.o_begin + o < a.TD)
+					__stcs(dst + o, ok ? acc[v][e] : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0));
+			}
+		__syncwarp();
+	}
+}
+
 // Active-node count per point (single grid).
 __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ FwdArgs a, long long* counts)
 {
@@ -924,22 +1232,29 @@ std::atomic<int> g_chunk_override{[]() { const char* e = getenv("SGI_CHUNK_ROWS"
 
 int chunk_rows_env() { return g_chunk_override.load(); }
 
-// FP32C variant of the direct entry points (plans time their own).
+// FP32C variant of the direct entry points (plans time their own);
+// sgi_set_fp32c_variant (or SGI_FP32C_VARIANT at start-up) overrides.
 constexpr int DEFAULT_VARIANT = 0;
-std::atomic<int> g_variant{DEFAULT_VARIANT};
+std::atomic<int> g_variant{[]() { const char* e = getenv("SGI_FP32C_VARIANT"); return e ? atoi(e) : DEFAULT_VARIANT; }()};
 
-// Forward kernel for a pass of `cols` outputs with row stride ld.  variant
-// (FP32C only) trades fine rows in flight per warp against warps per SM:
-// 0 = two rows, registers as needed; 1 = four rows, at least 3 blocks per SM;
-// 2 = two rows, at least 4 blocks per SM.  Plans time all three.
-// FP32C kernel variants (rows in flight per warp against warps per SM):
+uint32_t float_bits(float f)
+{
+	uint32_t u;
+	memcpy(&u, &f, 4);
+	return u;
+}
+
+// FP32C kernel variants (fine rows in flight per warp against warps per SM):
 // 0 = groups of four rows, at least 3 blocks per SM; 1 = two rows, 4 blocks;
-// 2 = eight rows, 2 blocks.  Plans time all of them.
+// 2 = eight rows, 2 blocks.  They run the descent walk when every grid of the
+// launch allows it (descent_ok), else the window walk; 3-5 force the window
+// walk with the settings of 0-2.  Plans time 0-2.
 constexpr int NVARIANTS = 3;
+constexpr int NVARIANTS_ALL = 6;
 template <int V, int E>
 void (*f32c_variant(int variant))(FwdArgs)
 {
-	switch (variant)
+	switch (variant % NVARIANTS)
 	{
 	case 1: return fwd_f32c_kernel<V, E, 2, 4>;
 	case 2: return fwd_f32c_kernel<V, E, 8, 2>;
@@ -947,22 +1262,43 @@ void (*f32c_variant(int variant))(FwdArgs)
 	}
 }
 
-void (*select_fwd(int precision, int ld, int cols, int variant = 0))(FwdArgs)
+template <int V, int E, bool FULLROW>
+void (*f32d_variant(int variant))(FwdArgs)
+{
+	switch (variant)
+	{
+	case 1: return fwd_f32d_kernel<V, E, 2, 4, FULLROW>;
+	case 2: return fwd_f32d_kernel<V, E, 8, 2, FULLROW>;
+	default: return fwd_f32d_kernel<V, E, 4, 3, FULLROW>;
+	}
+}
+
+template <int V, int E>
+void (*fp32c_kernel(int variant, bool descent, int cols))(FwdArgs)
+{
+	if (!descent || variant >= NVARIANTS) return f32c_variant<V, E>(variant);
+	// a pass whose columns fill every lane's outputs needs no column tests
+	return cols == V * 32 * E ? f32d_variant<V, E, true>(variant) : f32d_variant<V, E, false>(variant);
+}
+
+void (*select_fwd(int precision, int ld, int cols, int variant = 0, bool descent = false))(FwdArgs)
 {
 	const bool f64 = precision == SGI_FP64;
-	if (ld <= 32) return f64 ? fwd_f64_kernel<1, 1> : f32c_variant<1, 1>(variant);
-	if (cols <= 64) return f64 ? fwd_f64_kernel<1, 2> : f32c_variant<1, 2>(variant);
+	if (ld <= 32) return f64 ? fwd_f64_kernel<1, 1> : fp32c_kernel<1, 1>(variant, descent, cols);
+	if (cols <= 64) return f64 ? fwd_f64_kernel<1, 2> : fp32c_kernel<1, 2>(variant, descent, cols);
 	// FP32C reads four consecutive outputs per lane (16-byte loads) when rows
 	// are a multiple of 128 wide
 	const bool e4 = !f64 && ld % 128 == 0;
-	if (cols <= 128) return f64 ? fwd_f64_kernel<2, 2> : e4 ? f32c_variant<1, 4>(variant) : f32c_variant<2, 2>(variant);
-	return f64 ? fwd_f64_kernel<4, 2> : e4 ? f32c_variant<2, 4>(variant) : f32c_variant<4, 2>(variant);
+	if (cols <= 128)
+		return f64 ? fwd_f64_kernel<2, 2> : e4 ? fp32c_kernel<1, 4>(variant, descent, cols) : fp32c_kernel<2, 2>(variant, descent, cols);
+	return f64 ? fwd_f64_kernel<4, 2> : e4 ? fp32c_kernel<2, 4>(variant, descent, cols) : fp32c_kernel<4, 2>(variant, descent, cols);
 }
 
 // Dynamic shared memory of a forward launch.
-size_t fwd_smem(int precision, int dim)
+size_t fwd_smem(int precision, int dim, bool descent = false)
 {
-	return (size_t)WARPS * (precision == SGI_FP32C ? list_stride(dim) : dim) * sizeof(double);
+	if (precision != SGI_FP32C) return (size_t)WARPS * dim * sizeof(double);
+	return (size_t)WARPS * (descent ? desc_stride(dim) : list_stride(dim)) * sizeof(double);
 }
 
 int pick_R(int cols)
@@ -1003,10 +1339,16 @@ struct sgi_grid
 	double* s64c = nullptr;
 	uint32_t* coarse_index = nullptr;
 	int* parent = nullptr;
+	// descent layout (FP32C): child groups and per-node group ranges
+	uint4* grp_a = nullptr;
+	uint2* grp_b = nullptr;
+	uint4* ninfo = nullptr;
 	// host copy of the containment tree, for the ancestor chains of node
-	// chunk boundaries
+	// chunk boundaries, and of the group ranges and child bounds, for the
+	// descent's starts (pmax: running largest child index over a node's groups)
 	std::vector<int> parent_h;
 	std::vector<uint32_t> skip_h, depth_h;
+	std::vector<uint32_t> gfirst_h, gcount_h, gcmin_h, gpmax_h;
 	sgi_grid_info info{};
 };
 
@@ -1035,6 +1377,7 @@ void free_grid(sgi_grid* g)
 	cudaFree(g->parent);
 	cudaFree(g->rowmax);
 	cudaFree(g->aux);
+	cudaFree(g->grp_a); cudaFree(g->grp_b); cudaFree(g->ninfo);
 	cudaSetDevice(prev);
 	delete g;
 }
@@ -1051,6 +1394,7 @@ GridDesc desc_of(const sgi_grid* g, long long pt_begin, int precision = SGI_FP64
 	d.big_below = precision == SGI_FP32C ? (float)g->info.coarse_threshold : 0.f;
 	d.s64 = g->s64; d.s32 = g->s32; d.s64c = g->s64c;
 	d.coarse_index = g->coarse_index; d.parent = g->parent; d.pt_begin = pt_begin; d.nno = g->nno; d.ld = g->ld;
+	d.grp_a = g->grp_a; d.grp_b = g->grp_b; d.ninfo = g->ninfo; d.depth = g->info.tree_depth;
 	return d;
 }
 
@@ -1146,6 +1490,34 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 		}
 		if (!rc) rc = upload((void**)&d->rowmax, rmax.data(), rmax.size() * 4);
 		d->skip_below = (float)(ldexp(smax, -46));
+		// descent layout: groups, and per node (plus the roots' virtual
+		// parent at index nno) {first group, group count, rowmax, FP64 copy row}
+		DescentLayout D;
+		if (!rc) rc = build_descent(g, L, D);
+		if (!rc)
+		{
+			const size_t ng = D.cmin.size();
+			std::vector<uint32_t> ni((size_t)4 * (g.nno + 1));
+			for (int n = 0; n <= g.nno; n++)
+			{
+				ni[4 * (size_t)n + 0] = D.first[n];
+				ni[4 * (size_t)n + 1] = D.count[n];
+				ni[4 * (size_t)n + 2] = n < g.nno ? float_bits(rmax[n]) : 0u;
+				ni[4 * (size_t)n + 3] = n < g.nno ? L.lo_index[n] : DESC_NONE;
+			}
+			rc = upload((void**)&d->grp_a, D.a.data(), D.a.size() * 4);
+			if (!rc) rc = upload((void**)&d->grp_b, D.b.data(), D.b.size() * 4);
+			if (!rc) rc = upload((void**)&d->ninfo, ni.data(), ni.size() * 4);
+			d->gfirst_h = D.first;
+			d->gcount_h = D.count;
+			d->gcmin_h = D.cmin;
+			d->gpmax_h.resize(ng);
+			for (int n = 0; n <= g.nno; n++)
+			{
+				uint32_t m = 0;
+				for (uint32_t q = D.first[n]; q < D.first[n] + D.count[n]; q++) { m = std::max(m, D.cmax[q]); d->gpmax_h[q] = m; }
+			}
+		}
 	}
 	if (rc) { free_grid(d); return rc; }
 	sgi_grid_info& I = d->info;
@@ -1177,7 +1549,7 @@ extern "C" int sgi_set_chunk_rows(int rows)
 extern "C" int sgi_set_fp32c_variant(int variant)
 {
 	clear_error();
-	if (variant >= NVARIANTS) return fail(SGI_E_INVALID, "FP32C variant %d out of range (0..%d)", variant, NVARIANTS - 1);
+	if (variant >= NVARIANTS_ALL) return fail(SGI_E_INVALID, "FP32C variant %d out of range (0..%d)", variant, NVARIANTS_ALL - 1);
 	return g_variant.exchange(variant < 0 ? DEFAULT_VARIANT : variant);
 }
 
@@ -1233,6 +1605,55 @@ int chain_at(const sgi_grid* g, int c0, uint32_t* out)
 	return len;
 }
 
+// Group range of node n (n = nno: the roots' virtual parent) that may hold
+// children in [lo, hi): a node's groups are ordered by their smallest child,
+// so the range runs from the first group whose running largest child reaches
+// lo to the first group whose smallest child is at or past hi (a superset:
+// the kernel tests every child against the range).
+uint2 group_range(const sgi_grid* g, int n, int lo, int hi)
+{
+	const uint32_t b = g->gfirst_h[n], e = b + g->gcount_h[n];
+	const uint32_t* pm = g->gpmax_h.data();
+	const uint32_t* cm = g->gcmin_h.data();
+	const uint32_t s = (uint32_t)(std::lower_bound(pm + b, pm + e, (uint32_t)lo) - pm);
+	const uint32_t t = (uint32_t)(std::lower_bound(cm + b, cm + e, (uint32_t)hi) - cm);
+	return make_uint2(s, std::max(s, t));
+}
+
+// Walk starts of a launch over grids[gb .. gb + ng) for the node range set in
+// a (chunk_begin, chunk_len): the ancestor chain of the range start and, for
+// the descent layout, the group ranges of the chain nodes and of the roots.
+void set_starts(FwdArgs& a, const sgi_grid_t* grids, int gb, int ng)
+{
+	for (int k = 0; k < ng; k++)
+	{
+		const sgi_grid* g = grids[gb + k];
+		a.chain_len[k] = chain_at(g, a.chunk_begin, a.chain[k]);
+		a.rseg[k] = make_uint2(0u, 0u);
+		if (g->gfirst_h.empty()) continue;
+		const int lo = a.chunk_begin;
+		const int hi = a.chunk_len ? (int)std::min((long long)g->nno, (long long)a.chunk_begin + a.chunk_len) : g->nno;
+		if (lo >= hi) continue;
+		a.rseg[k] = group_range(g, g->nno, lo, hi);
+		for (int d = 0; d < a.chain_len[k]; d++) a.cseg[k][d] = group_range(g, (int)a.chain[k][d], lo, hi);
+	}
+}
+
+// The FP32C descent needs every grid of the launch to have its layout and a
+// tree shallow enough for the stack bound, and for chunked launches for
+// complete ancestor chains.
+bool descent_ok(const sgi_grid_t* grids, int gb, int ng, bool chunked)
+{
+	for (int k = 0; k < ng; k++)
+	{
+		const sgi_grid* g = grids[gb + k];
+		if (!g->grp_a || g->gfirst_h.empty()) return false;
+		const int dep = g->info.tree_depth;
+		if (dep > SCAP - 32 || (chunked && dep > CHAIN + 1)) return false;
+	}
+	return true;
+}
+
 // Launches of one forward call.  chunk < 0: the automatic chunk size; work
 // counters come from `counters` (one per launch, in order) when given, else
 // from the device workspace's ring.
@@ -1248,10 +1669,9 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 	if (precision == SGI_FP64) { for (int k = 0; k < ngrids; k++) if (!grids[k]->s64) return fail(SGI_E_INVALID, "grid %d has no FP64 surplus", k); }
 	else if (precision == SGI_FP32C) { for (int k = 0; k < ngrids; k++) if (!grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k); }
 	else return fail(SGI_E_INVALID, "unknown precision %d", precision);
-	// per warp: the point's coordinates, and for FP32C the weight stack (and
-	// the list form's term list)
-	const size_t smem = fwd_smem(precision, g0->dim);
-	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
+	// per warp: the point's coordinates, and for FP32C the term list and the
+	// weight stack (window walk) or the group-range stack (descent)
+	if (fwd_smem(precision, g0->dim, true) > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	g_stats = sgi_launch_stats{};
 	int launches = 0;
 	for (int gb = 0; gb < ngrids; gb += MAXG)
@@ -1270,16 +1690,18 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 		for (int k = 0; k < ng; k++) maxnno = std::max(maxnno, grids[gb + k]->nno);
 		const int clen = chunk < 0 ? chunk_rows(W, g0, precision, a.npts, maxnno) : (chunk >= maxnno ? 0 : chunk);
 		const int nchunks = clen ? (maxnno + clen - 1) / clen : 1;
+		const bool descent = precision == SGI_FP32C && descent_ok(grids, gb, ng, clen > 0);
+		const size_t smem = fwd_smem(precision, g0->dim, descent);
 		for (int ob = 0; ob < g0->TD; ob += PASS)
 		for (int c = 0; c < std::max(nchunks, 1); c++)
 		{
 			a.o_begin = ob;
 			a.chunk_begin = c * clen;
 			a.chunk_len = clen;
-			for (int k = 0; k < ng; k++) a.chain_len[k] = chain_at(grids[gb + k], a.chunk_begin, a.chain[k]);
+			set_starts(a, grids, gb, ng);
 			a.counter = counters ? counters + launches : W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant);
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant, descent);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, W->sms, &blocks);
@@ -1585,8 +2007,7 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 	}
 	const sgi_grid* g0 = grids[0];
 	const int variant = 0;
-	const size_t smem = fwd_smem(precision, g0->dim);
-	if (smem > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
+	if (fwd_smem(precision, g0->dim, true) > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	// count the launches first: reject before launching anything
 	const int passes = (g0->TD + PASS - 1) / PASS;
 	long long launches = 0;
@@ -1616,12 +2037,15 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		a.out = out + (size_t)p0 * g0->TD;
 		a.npts = p1 - p0;
 		a.ngrids = ng; a.dim = g0->dim; a.TD = g0->TD;
+		set_starts(a, grids, gb, ng);   // whole grids: the roots' groups
+		const bool descent = precision == SGI_FP32C && descent_ok(grids, gb, ng, false);
+		const size_t smem = fwd_smem(precision, g0->dim, descent);
 		for (int ob = 0; ob < g0->TD; ob += PASS)
 		{
 			a.o_begin = ob;
 			a.counter = counters + slot++;
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant);
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant, descent);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, sms, &blocks);

@@ -857,7 +857,117 @@ int build_layout(const HostGrid& g, DeviceLayout& L)
 	return SGI_OK;
 }
 
+int build_descent(const HostGrid& g, const DeviceLayout& L, DescentLayout& D)
+{
+	const int nno = g.nno;
+	// children of every node in index order; index nno collects the roots
+	std::vector<uint32_t> kid_ptr(nno + 2, 0), kids;
+	for (int n = 0; n < nno; n++)
+	{
+		if (L.rec[4 * (size_t)n + 2] & NODE_DEAD) continue;
+		const int p = L.parent[n] < 0 ? nno : L.parent[n];
+		kid_ptr[p + 1]++;
+	}
+	for (int p = 0; p <= nno; p++) kid_ptr[p + 1] += kid_ptr[p];
+	kids.assign(kid_ptr[nno + 1], 0);
+	{
+		std::vector<uint32_t> fill(kid_ptr.begin(), kid_ptr.end() - 1);
+		for (int n = 0; n < nno; n++)
+		{
+			if (L.rec[4 * (size_t)n + 2] & NODE_DEAD) continue;
+			const int p = L.parent[n] < 0 ? nno : L.parent[n];
+			kids[fill[p]++] = (uint32_t)n;
+		}
+	}
+	D.a.clear(); D.b.clear(); D.cmin.clear(); D.cmax.clear();
+	D.first.assign(nno + 1, 0);
+	D.count.assign(nno + 1, 0);
+	D.npairs = 0;
+	struct Grp { uint32_t L, R, dk, old, ijL, ijR, lo, hi; };
+	std::vector<Grp> grp;
+	std::vector<std::pair<uint32_t, uint32_t>> simple;   // (delta dim, child)
+	for (int p = 0; p <= nno; p++)
+	{
+		grp.clear();
+		simple.clear();
+		for (uint32_t a = kid_ptr[p]; a < kid_ptr[p + 1]; a++)
+		{
+			const uint32_t c = kids[a];
+			const uint32_t z = L.rec[4 * (size_t)c + 2];
+			if (z & NODE_MULTI) grp.push_back({ c, DESC_NONE, DESC_MULTI << 16, 0u, 0u, 0u, c, c });
+			else if (z & NODE_ALWAYS) grp.push_back({ c, DESC_NONE, DESC_ALWAYS << 16, 0u, 0u, 0u, c, c });
+			else simple.emplace_back(z >> 16, c);
+		}
+		// simple children by dimension: exactly two in a dimension with
+		// disjoint supports there form a pair, every other one is a singleton
+		std::sort(simple.begin(), simple.end());
+		for (size_t s = 0; s < simple.size();)
+		{
+			size_t e = s + 1;
+			while (e < simple.size() && simple[e].first == simple[s].first) e++;
+			const uint32_t dd = simple[s].first;
+			bool paired = false;
+			if (e - s == 2)
+			{
+				const uint32_t c = simple[s].second, c2 = simple[s + 1].second;
+				const uint32_t ij = L.rec[4 * (size_t)c + 3], ij2 = L.rec[4 * (size_t)c2 + 3];
+				const uint32_t old = L.aux[2 * (size_t)c];
+				const int64_t i1 = ij & 0xffff, j1 = ij >> 16, i2 = ij2 & 0xffff, j2 = ij2 >> 16;
+				// open supports ((j-1)/i, (j+1)/i): the left one ends where or
+				// before the right one starts
+				const bool c_left = (j1 + 1) * i2 <= (j2 - 1) * i1;
+				const bool c2_left = (j2 + 1) * i1 <= (j1 - 1) * i2;
+				if ((c_left || c2_left) && L.aux[2 * (size_t)c2] == old)
+				{
+					grp.push_back({ c_left ? c : c2, c_left ? c2 : c, dd, old, c_left ? ij : ij2, c_left ? ij2 : ij,
+					                std::min(c, c2), std::max(c, c2) });
+					D.npairs++;
+					paired = true;
+				}
+			}
+			if (!paired)
+				for (size_t k = s; k < e; k++)
+				{
+					const uint32_t c = simple[k].second;
+					grp.push_back({ c, DESC_NONE, dd, L.aux[2 * (size_t)c], L.rec[4 * (size_t)c + 3], 0u, c, c });
+				}
+			s = e;
+		}
+		std::stable_sort(grp.begin(), grp.end(), [](const Grp& x, const Grp& y) { return x.lo < y.lo; });
+		D.first[p] = (uint32_t)D.cmin.size();
+		D.count[p] = (uint32_t)grp.size();
+		for (const Grp& q : grp)
+		{
+			D.a.insert(D.a.end(), { q.L, q.R, q.dk, q.old });
+			D.b.insert(D.b.end(), { q.ijL, q.ijR });
+			D.cmin.push_back(q.lo);
+			D.cmax.push_back(q.hi);
+		}
+	}
+	return SGI_OK;
+}
+
 } // namespace sgi
+
+extern "C" int sgi_host_grid_descent(sgi_host_grid_t hg, int* ngroups, int* npairs, uint32_t* a, uint32_t* b,
+	uint32_t* first, uint32_t* count)
+{
+	clear_error();
+	if (!hg || !ngroups) return fail(SGI_E_INVALID, "null argument");
+	DeviceLayout L;
+	int rc = build_layout(hg->g, L);
+	if (rc) return rc;
+	DescentLayout D;
+	rc = build_descent(hg->g, L, D);
+	if (rc) return rc;
+	*ngroups = (int)D.cmin.size();
+	if (npairs) *npairs = D.npairs;
+	if (a) memcpy(a, D.a.data(), D.a.size() * 4);
+	if (b) memcpy(b, D.b.data(), D.b.size() * 4);
+	if (first) memcpy(first, D.first.data(), D.first.size() * 4);
+	if (count) memcpy(count, D.count.data(), D.count.size() * 4);
+	return SGI_OK;
+}
 
 extern "C" int sgi_host_grid_tree(sgi_host_grid_t hg, int* skip, int* parent)
 {

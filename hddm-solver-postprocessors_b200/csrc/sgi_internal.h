@@ -57,6 +57,39 @@ struct DeviceLayout
 // Builds the containment tree over the grid's node order and the records.
 int build_layout(const HostGrid& g, DeviceLayout& L);
 
+// ------------------------------------------------------- descent layout
+//
+// The FP32C walk descends the containment tree from the active nodes only.
+// The tree children of a node are split into groups:
+//   * a pair: two children that differ from the node in the same dimension d
+//     only, with disjoint supports in d (the left and right halves of the
+//     node's support at the next level) — at most one of them is active at a
+//     point, and the point's coordinate picks which;
+//   * a singleton: any other child.
+// Group g (arrays of ngroups entries):
+//   a[g] = {L, R (NONE for a singleton), d | kind << 16, parent's (i | j << 16)
+//           in d (0 when the parent is constant there)}
+//   b[g] = {L's (i | j << 16) in d, R's}
+// kind: DESC_SIMPLE (L/R differ from the parent in d only), DESC_MULTI (L
+// differs in several dimensions: all its components are checked),
+// DESC_ALWAYS (L has the parent's components: active with the parent).
+// Node n's groups are [first[n], first[n] + count[n]), ordered by their
+// smallest child index; entry nno is a virtual parent of the tree roots.
+constexpr uint32_t DESC_NONE = 0xffffffffu;
+enum DescKind : uint32_t { DESC_SIMPLE = 0, DESC_MULTI = 1, DESC_ALWAYS = 2 };
+
+struct DescentLayout
+{
+	std::vector<uint32_t> a;        // 4 per group
+	std::vector<uint32_t> b;        // 2 per group
+	std::vector<uint32_t> first;    // nno + 1
+	std::vector<uint32_t> count;    // nno + 1
+	std::vector<uint32_t> cmin, cmax; // smallest / largest child index per group
+	int npairs = 0;
+};
+
+int build_descent(const HostGrid& g, const DeviceLayout& L, DescentLayout& D);
+
 // Rows whose largest |surplus| is at least this keep an FP64 copy for the
 // FP32C form's big terms (2^-16 of the grid's largest |surplus|, or
 // SGI_COARSE_REL times it).

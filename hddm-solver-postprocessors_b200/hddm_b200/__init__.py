@@ -62,6 +62,7 @@ def _load():
         "sgi_host_grid_free": (None, [P]),
         "sgi_host_grid_xps_chains": (I, [P, _c_int_p, _c_int_p, P, P, P]),
         "sgi_host_grid_tree": (I, [P, P, P]),
+        "sgi_host_grid_descent": (I, [P, _c_int_p, _c_int_p, P, P, P, P]),
         "sgi_gen_regular": (I, [I, I, I, U64, ctypes.POINTER(P)]),
         "sgi_gen_adaptive": (I, [I, I, I, I, D, U64, ctypes.POINTER(P)]),
         "sgi_gen_points": (I, [I, ctypes.c_long, I, U64, D, I, P]),
@@ -108,7 +109,7 @@ class HostGrid:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.sgi_host_grid_free(h)
             self._h = None
 
@@ -198,6 +199,21 @@ class HostGrid:
         return skip, parent
 
 
+    def descent(self):
+        """Child groups of the FP32C descent: (a [ngroups, 4], b [ngroups, 2],
+        first [nno + 1], count [nno + 1], npairs), uint32."""
+        ng, npr = ctypes.c_int(), ctypes.c_int()
+        _check(lib.sgi_host_grid_descent(self._h, ctypes.byref(ng), ctypes.byref(npr), None, None, None, None))
+        nno = self.nno
+        a = np.zeros((ng.value, 4), np.uint32)
+        b = np.zeros((ng.value, 2), np.uint32)
+        first = np.zeros(nno + 1, np.uint32)
+        count = np.zeros(nno + 1, np.uint32)
+        _check(lib.sgi_host_grid_descent(self._h, ctypes.byref(ng), ctypes.byref(npr), a.ctypes.data,
+                                         b.ctypes.data, first.ctypes.data, count.ctypes.data))
+        return a, b, first, count, npr.value
+
+
 def gen_points(dim, npts, kind=0, seed=0, kink_reject=0.0, max_level=7):
     out = np.zeros((npts, dim), np.float64)
     _check(lib.sgi_gen_points(dim, npts, kind, seed, kink_reject, max_level, out.ctypes.data))
@@ -226,7 +242,7 @@ class Grid:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.sgi_grid_destroy(h)
             self._h = None
 
@@ -339,7 +355,7 @@ class Plan:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.sgi_plan_destroy(h)
             self._h = None
 

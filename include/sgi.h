@@ -109,6 +109,21 @@ int sgi_host_grid_xps_chains(sgi_host_grid_t g, int* nfreqs, int* szxps,
  * and n's subtree is the index range [n, skip[n]).  No reference counterpart. */
 int sgi_host_grid_tree(sgi_host_grid_t g, int* skip, int* parent);
 
+/* The child groups the FP32C descent walks (for inspection and tests).  The
+ * tree children of each node are grouped: two children that differ from the
+ * node only in the same dimension d, with disjoint supports in d, form a pair
+ * (at most one is active at any point, and x_d picks it); every other child is
+ * a singleton.  Group g: a[4g..4g+3] = {left child, right child (0xffffffff
+ * for a singleton), d | kind << 16, the parent's (i | j << 16) in d (0 when
+ * constant)}, b[2g..2g+1] = {left's (i | j << 16) in d, right's}; kind 0 =
+ * the children differ from the parent in d only, 1 = the child differs in
+ * several dimensions, 2 = the child has the parent's components.  Node n's
+ * groups are [first[n], first[n] + count[n]); entry nno lists the tree roots.
+ * Call with null arrays first to get ngroups; a is 4*ngroups, b 2*ngroups,
+ * first and count nno + 1 entries.  No reference counterpart. */
+int sgi_host_grid_descent(sgi_host_grid_t g, int* ngroups, int* npairs, uint32_t* a, uint32_t* b,
+	uint32_t* first, uint32_t* count);
+
 /* --------------------------------------------------------- device grids */
 typedef struct sgi_grid* sgi_grid_t;
 
@@ -207,13 +222,17 @@ int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* o
  * setting.  No reference counterpart. */
 int sgi_set_chunk_rows(int rows);
 
-/* FP32C kernel variant used by sgi_interpolate and sgi_interpolate_host
- * (plans pick their own by timing): 0 = four surplus rows in flight per warp,
- * 1 = two rows and more warps per SM, 2 = eight rows and fewer warps.  The
- * variants interleave the FP64 additions of big terms and of FP32 partial
- * sums differently, so their results may differ in the last bits (all within
- * the FP32C tolerance).  variant < 0 restores the default (0).  Returns the
- * previous setting, or a negative error code.  No reference counterpart. */
+/* FP32C kernel variant used by sgi_interpolate, sgi_interpolate_host and
+ * sgi_interpolate_noalloc (plans pick their own by timing among 0-2): 0 = four
+ * fine surplus rows in flight per warp, 1 = two rows and more warps per SM,
+ * 2 = eight rows and fewer warps.  Variants 0-2 walk the tree by descent
+ * (child groups, see sgi_host_grid_descent) whenever every grid of a launch
+ * allows it (tree depth <= 96, and <= 32 for node-chunked launches), else by
+ * node windows; 3-5 are 0-2 with the node-window walk forced.  The variants
+ * order the FP64 additions of big terms and of FP32 partial sums differently,
+ * so their results may differ in the last bits (all within the FP32C
+ * tolerance).  variant < 0 restores the default (0).  Returns the previous
+ * setting, or a negative error code.  No reference counterpart. */
 int sgi_set_fp32c_variant(int variant);
 
 /* Plans: one forward call recorded into a CUDA graph and replayed.
@@ -235,9 +254,8 @@ typedef struct sgi_plan* sgi_plan_t;
 int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
 	const double* x, double* out, int precision, int chunk_rows, void* stream, sgi_plan_t* plan);
 int sgi_plan_launch(sgi_plan_t plan, void* stream);
-/* The plan's node-chunk size, kernel variant (FP32C: 0 = two fine rows in
- * flight per warp, 1 = four rows at >= 3 blocks per SM, 2 = two rows at >= 4
- * blocks per SM), launches per replay and the tuned time of one call (ms). */
+/* The plan's node-chunk size, FP32C kernel variant (as sgi_set_fp32c_variant),
+ * launches per replay and the tuned time of one call (ms). */
 int sgi_plan_info(sgi_plan_t plan, int* chunk_rows, int* variant, int* launches, float* tuned_ms);
 void sgi_plan_destroy(sgi_plan_t plan);
 

@@ -181,3 +181,165 @@ def test_grid_create_without_gpu_fails_cleanly():
     with pytest.raises(H.SgiError) as e:
         H.Grid(H.HostGrid.regular(4, 2, 2, 0))
     assert e.value.code == -7
+
+
+def _hat(x, ij):
+    i = np.float64(int(ij) & 0xFFFF)
+    j = np.float64(int(ij) >> 16)
+    return 1.0 - abs(x * i - j)
+
+
+def _descend(desc, x, lo, hi, starts, act, wfull):
+    """The FP32C descent over the exported child groups for one point: from
+    the start segments (group range, parent weight), every group yields at
+    most one active child; hits outside [lo, hi) are not kept or expanded."""
+    a, b, first, count, _ = desc
+    hits = {}
+    stack = list(starts)
+    while stack:
+        gb, ge, wp = stack.pop()
+        for g in range(gb, ge):
+            kind, d = (int(a[g, 2]) >> 16) & 3, int(a[g, 2]) & 0xFFFF
+            c, w = None, None
+            if kind == 0:
+                h = _hat(x[d], b[g, 0])
+                if h > 0:
+                    c = int(a[g, 0])
+                elif a[g, 1] != 0xFFFFFFFF:
+                    h = _hat(x[d], b[g, 1])
+                    if h > 0:
+                        c = int(a[g, 1])
+                if c is not None:
+                    w = wp * h / (_hat(x[d], a[g, 3]) if a[g, 3] else 1.0)
+            elif kind == 1:
+                # several changed dimensions: every component is checked
+                c = int(a[g, 0])
+                c, w = (c, wfull[c]) if act[c] else (None, None)
+            else:
+                c, w = int(a[g, 0]), wp
+            if c is None or not (lo <= c < hi):
+                continue
+            assert c not in hits
+            hits[c] = w
+            if count[c] and c + 1 < hi:
+                stack.append((int(first[c]), int(first[c] + count[c]), w))
+    return hits
+
+
+@pytest.mark.parametrize("kind", ["regular", "adaptive", "shuffled", "fixture"])
+def test_descent_groups_reach_exactly_the_active_nodes(kind):
+    """Every node whose hats are all positive is reached exactly once, from
+    the roots or from the active ancestors of a node-range start, with the
+    weight of the full product; no other node is reached."""
+    if kind == "regular":
+        g, dim = H.HostGrid.regular(6, 4, 2, 0), 6
+    elif kind == "adaptive":
+        g, dim = H.HostGrid.adaptive(20, 3000, 2, 5), 20
+    elif kind == "shuffled":
+        idx, sur = H.HostGrid.adaptive(12, 1500, 2, 6).arrays()
+        perm = np.random.default_rng(0).permutation(len(idx))
+        g, dim = H.HostGrid.from_dense(idx[perm], sur[perm]), 12
+    else:
+        g, dim = H.HostGrid.read_plt(PLT, 59), 59
+    desc = g.descent()
+    a, b, first, count, npairs = desc
+    idx, _ = g.arrays()
+    skip, parent = g.tree()
+    n = len(skip)
+    assert len(first) == n + 1 and a.shape[0] == count.sum()
+    if kind != "shuffled":
+        assert npairs > 0
+    i = idx[:, :dim].astype(np.float64)
+    j = idx[:, dim:].astype(np.float64)
+    X = H.gen_points(dim, 12, kind=2, seed=7)
+    rng = np.random.default_rng(1)
+    ranges = [(0, n)] + [tuple(sorted(rng.choice(n + 1, 2, replace=False))) for _ in range(4)]
+    for x in X:
+        h = 1.0 - np.abs(x[None, :] * i - j)
+        nz = (i != 0) | (j != 0)
+        act = np.all(np.where(nz, h > 0, True), axis=1)
+        wfull = np.prod(np.where(nz, h, 1.0), axis=1)
+        for lo, hi in ranges:
+            starts = [(int(first[n]), int(first[n] + count[n]), 1.0)]
+            if lo > 0:
+                # the strict ancestors of lo: the groups of the active ones start the range
+                q = lo - 1
+                while q >= 0 and skip[q] <= lo:
+                    q -= 1
+                chain = []
+                while q >= 0:
+                    if skip[q] > lo:
+                        chain.append(q)
+                    q = parent[q]
+                # activity along the ancestor path is monotone (nested
+                # supports): the active ones are the shallowest
+                starts += [(int(first[c]), int(first[c] + count[c]), wfull[c]) for c in chain if act[c]]
+            hits = _descend(desc, x, lo, hi, starts, act, wfull)
+            want = {c for c in range(lo, hi) if act[c]}
+            assert set(hits) == want, (kind, lo, hi)
+            for c, w in hits.items():
+                assert abs(w - wfull[c]) <= 1e-13 * max(1.0, abs(wfull[c]))
+
+
+SCAP = 128  # descent stack entries per warp (fwd_f32d_kernel)
+
+
+def _stack_peak(desc, x, depth, lo=0, hi=None):
+    """Largest stack size of the descent kernel's stepping rule for one point:
+    each step takes up to 32 groups from the top ranges (one group when
+    size + 32 + depth > SCAP), ranges taken whole are popped, the range taken
+    in part keeps its remainder, and every hit with children pushes a range."""
+    a, b, first, count, _ = desc
+    n = len(first) - 1
+    hi = n if hi is None else hi
+    stack = [[int(first[n]), int(first[n] + count[n])]]
+    peak = len(stack)
+    while stack:
+        B = 32 if len(stack) + 32 + depth <= SCAP else 1
+        taken, take = [], B
+        while take and stack:
+            gb, ge = stack[-1]
+            k = min(take, ge - gb)
+            taken += range(gb, gb + k)
+            take -= k
+            if gb + k == ge:
+                stack.pop()
+            else:
+                stack[-1][0] = gb + k
+        for g in taken:
+            kind, d = (int(a[g, 2]) >> 16) & 3, int(a[g, 2]) & 0xFFFF
+            c = None
+            if kind == 0:
+                if _hat(x[d], b[g, 0]) > 0:
+                    c = int(a[g, 0])
+                elif a[g, 1] != 0xFFFFFFFF and _hat(x[d], b[g, 1]) > 0:
+                    c = int(a[g, 1])
+            else:
+                c = int(a[g, 0])
+            if c is not None and lo <= c < hi and count[c] and c + 1 < hi:
+                stack.append([int(first[c]), int(first[c] + count[c])])
+        peak = max(peak, len(stack))
+    return peak
+
+
+@pytest.mark.parametrize("kind", ["regular_wide", "adaptive", "fixture"])
+def test_descent_stack_stays_within_capacity(kind):
+    """The descent kernel's stack bound (depth <= SCAP - 32): replaying its
+    stepping rule on grids with many children per node never needs more than
+    SCAP entries."""
+    if kind == "regular_wide":
+        g, dim = H.HostGrid.regular(40, 3, 1, 0), 40
+    elif kind == "adaptive":
+        g, dim = H.HostGrid.adaptive(59, 20000, 1, 4), 59
+    else:
+        g, dim = H.HostGrid.read_plt(PLT, 59), 59
+    desc = g.descent()
+    _, parent = g.tree()
+    depth = 1
+    dep = np.zeros(len(parent), np.int64)
+    for c in range(len(parent)):
+        dep[c] = 1 if parent[c] < 0 else dep[parent[c]] + 1
+    depth = int(dep.max())
+    assert depth <= SCAP - 32
+    for x in H.gen_points(dim, 8, kind=2, seed=3):
+        assert _stack_peak(desc, x, depth) <= SCAP
