@@ -726,20 +726,27 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32c_kernel(const __grid_cons
 // weight times its hat over the parent's hat in that dimension; a hit with
 // children in the launch's node range pushes its own group range.
 //
-// Stack bound: a step takes 32 groups while size + 32 + depth <= SCAP (depth
-// = the tree's depth), else one group from the top range.  A 32-group step
-// pushes at most 32 ranges, so it leaves at most SCAP - depth.  Single-group
-// steps push, above the ranges present when they began, a chain of ranges of
-// increasing tree depth (each one the children of a node taken from the range
-// below it): at most depth of them.  The starts are at most 32 ranges (the
-// roots' and one per chain node), so the size stays within SCAP whenever
+// Stack bound: a step takes B = min(32, SCAP - depth - size) groups (depth =
+// the tree's depth), or one group from the top range when that is below 1.
+// A step of B groups pushes at most B ranges, so it leaves at most
+// SCAP - depth.  Single-group steps push, above the ranges present when they
+// began (at most SCAP - depth), a chain of ranges of increasing tree depth
+// (each one the children of a node taken from the range below it): at most
+// depth of them, so the size never exceeds SCAP.  The starts are at most 32
+// ranges (the roots' and one per chain node), which fit while
 // depth <= SCAP - 32.  The host selects this kernel only then, and for
 // chunked launches only when every chain is complete (depth <= CHAIN + 1).
-constexpr int SCAP = 128;
+// SCAP = 96 keeps the shared memory per warp small (what the blocks do not
+// take stays L1 cache, which holds re-read surplus rows) while steps of 32
+// groups stay the rule: on the d=59, 1M-node grid the stack holds at most
+// about 40 ranges.
+constexpr int SCAP = 96;
 
 // Shared memory per warp of the descent form, in doubles: the stack (SCAP
-// 16-byte entries), the fine-term list, the chain weights and the point.
-__host__ __device__ __forceinline__ int desc_stride(int dim) { return 2 * SCAP + FCAP + 32 + ((dim + 1) & ~1); }
+// 16-byte entries), the fine-term list (whose first 32 doubles hold the chain
+// weights at a chunk start, before any term is listed) and the point.
+__host__ __device__ __forceinline__ int desc_stride(int dim) { return 2 * SCAP + FCAP + ((dim + 1) & ~1); }
+static_assert(FCAP >= 32, "the chain weights (32 doubles) alias the fine-term list");
 
 __device__ __forceinline__ uint4 pack_seg(uint32_t b, uint32_t e, double w)
 {
@@ -756,8 +763,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 	double* wbase = smem + (threadIdx.x >> 5) * desc_stride(a.dim);
 	uint4* stk = reinterpret_cast<uint4*>(wbase);
 	uint2* fl = reinterpret_cast<uint2*>(wbase + 2 * SCAP);
-	double* wchain = wbase + 2 * SCAP + FCAP;
-	double* xs = wchain + 32;
+	double* wchain = wbase + 2 * SCAP;     // aliases fl: used before any term is listed
+	double* xs = wbase + 2 * SCAP + FCAP;
 	const bool first = a.chunk_begin == 0;
 	for (;;)
 	{
@@ -812,7 +819,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 			const double* s64l = G.s64c + lcol;
 			const uint32_t ld = (uint32_t)G.ld;
 			const float skip_below = G.skip_below, big_below = G.big_below;
-			const int bmax = SCAP - 32 - G.depth;   // 32-group steps while size <= bmax
+			const int room = SCAP - G.depth;        // steps of min(32, room - size) groups
 			float part[V][E];
 #pragma unroll
 			for (int v = 0; v < V; v++)
@@ -865,7 +872,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 			};
 			while (size > 0)
 			{
-				const int B = size <= bmax ? 32 : 1;
+				const int B = max(1, min(32, room - size));
 				// lane k looks at stack entry size - 1 - k (lane 0: the top)
 				uint4 e = make_uint4(0u, 0u, 0u, 0u);
 				if (lane < size) e = stk[size - 1 - lane];

@@ -281,21 +281,21 @@ def test_descent_groups_reach_exactly_the_active_nodes(kind):
                 assert abs(w - wfull[c]) <= 1e-13 * max(1.0, abs(wfull[c]))
 
 
-SCAP = 128  # descent stack entries per warp (fwd_f32d_kernel)
+SCAP = 96  # descent stack entries per warp (fwd_f32d_kernel)
 
 
 def _stack_peak(desc, x, depth, lo=0, hi=None):
     """Largest stack size of the descent kernel's stepping rule for one point:
-    each step takes up to 32 groups from the top ranges (one group when
-    size + 32 + depth > SCAP), ranges taken whole are popped, the range taken
-    in part keeps its remainder, and every hit with children pushes a range."""
+    each step takes min(32, SCAP - depth - size) groups (at least one) from
+    the top ranges, ranges taken whole are popped, the range taken in part
+    keeps its remainder, and every hit with children pushes a range."""
     a, b, first, count, _ = desc
     n = len(first) - 1
     hi = n if hi is None else hi
     stack = [[int(first[n]), int(first[n] + count[n])]]
     peak = len(stack)
     while stack:
-        B = 32 if len(stack) + 32 + depth <= SCAP else 1
+        B = max(1, min(32, SCAP - depth - len(stack)))
         taken, take = [], B
         while take and stack:
             gb, ge = stack[-1]
