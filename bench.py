@@ -77,9 +77,9 @@ def alg_bytes(hg, info, npts, s_b):
 GATHER_PEAK_TBS = 18.7
 
 # DRAM bytes (read + write) of one FP32C step of the default workload: the sum
-# over the four fwd_f32c_kernel launches of one graph replay in an ncu capture
-# (profiles/fwd_f32c_c4_traffic.md).
-FP32C_STEP_DRAM_BYTES = 270.2e9
+# over the 16 fwd_f32d_kernel launches (node chunks of 64,768) of one forward
+# call in an ncu capture (profiles/fwd_f32d_c4_traffic.md).
+FP32C_STEP_DRAM_BYTES = 48.9e9
 
 
 def gather_roof(mean_active, ms, grid, hg):
@@ -185,15 +185,17 @@ def run_gpu(args):
         return total, per, plan.launches
 
     if args.profile_replay:
-        # one warm-up and one measured replay of the FP32C plan (the timed
-        # step), nothing else: the case a launch-level capture looks at
-        chunk = args.chunk_rows if args.chunk_rows >= 0 else 259072
-        plan = H.Plan(grid, x, out32, precision=H.FP32C, chunk_rows=chunk, stream=stream)
-        plan.launch(stream=stream)
-        plan.launch(stream=stream)
+        # two FP32C forward calls (a warm-up and a measured one) with a fixed
+        # node-chunk size and kernel variant, nothing else: the case a
+        # launch-level capture looks at (skip the first call's launches)
+        chunk = args.chunk_rows if args.chunk_rows >= 0 else 64768
+        H.set_chunk_rows(chunk)
+        H.set_fp32c_variant(args.variant)
+        for _ in range(2):
+            H.interpolate(grid, x, precision=H.FP32C, out=out32, stream=stream)
         torch.cuda.synchronize(dev)
-        print(json.dumps({"profile_replay": {"chunk_rows": plan.chunk_rows, "variant": plan.variant,
-                                             "launches": plan.launches}}))
+        print(json.dumps({"profile_replay": {"chunk_rows": chunk, "variant": args.variant,
+                                             "launches_per_call": H.last_launch().kernels}}))
         return
     # accuracy of the FP32C form against the FP64 form (bit-identical to gold), all points
     H.interpolate(grid, x, precision=H.FP64, out=out64, stream=stream)
@@ -293,7 +295,9 @@ def run_gpu(args):
             "fp32c_vs_gold_exact_fp64": {"max_rel_err": err_max, "rms_rel_err": err_rms, "points": npts},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                          "peak_kind": f"{peak_kind} (burst copy)", "algorithmic_bytes_per_launch": b32,
-                         "traffic": traffic, "kernel": "fwd_f32c_kernel"},
+                         "traffic": traffic, "kernel": "fwd_f32d_kernel",
+                         "traffic_note": "ncu DRAM read+write of one forward call with node chunks of 64,768 "
+                                         "(16 launches); the timed plan's chunking is in plans.fp32c"},
             "gather_roofline": gather_roof(mean_active, ms32, grid, hg),
             "walk_only_ms": walk_ms,
             "fma_work": {"mean_active_nodes": mean_active,
@@ -572,6 +576,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=NPTS, help="points per GPU (default: the workload's 1M)")
     ap.add_argument("--chunk-rows", type=int, default=-1, help="node-chunk size of the plans (-1: autotune)")
+    ap.add_argument("--variant", type=int, default=1, help="--profile-replay: FP32C kernel variant")
     ap.add_argument("--profile-replay", action="store_true",
                     help="only run two replays of the FP32C plan (launch-level profiling case)")
     ap.add_argument("--only-accuracy-pass", action="store_true",
