@@ -87,3 +87,17 @@ def test_backward_empty_and_no_outputs(cuda):
     x = torch.zeros((0, 4), dtype=torch.float64, device="cuda")
     gx, gs = H.backward(g, x, torch.zeros((0, 8), dtype=torch.float64, device="cuda"))
     assert gx.shape == (0, 4) and float(gs.abs().sum()) == 0.0
+
+
+def test_sharded_backward_single_rank_is_the_kernel(cuda):
+    """Without a process group, backward_sharded is the GPU backward itself."""
+    import torch
+    from hddm_b200.shard import backward_sharded
+    hg = H.HostGrid.adaptive(16, 3000, 32, seed=8)
+    g = H.Grid(hg)
+    X = H.gen_points(16, 128, kind=0, seed=9, kink_reject=1e-6)
+    C = np.random.default_rng(3).standard_normal((128, 32))
+    x, c = torch.from_numpy(X).cuda(), torch.from_numpy(C).cuda()
+    gx, gs = backward_sharded(g, x, c)
+    rx, rs = H.backward(g, x, c)
+    assert torch.equal(gx, rx) and torch.equal(gs, rs)

@@ -73,3 +73,55 @@ def test_two_rank_gloo_shard_and_gather():
         assert p.exitcode == 0
     equal, timed = ret.get(timeout=10)
     assert equal and timed
+
+
+def _bwd_worker(rank, world, port, ret):
+    import sys
+    import torch
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in (root, os.path.join(root, "hddm-solver-postprocessors_b200")):
+        sys.path.insert(0, p)
+    import hddm_b200 as H
+    import oracle as O
+    from hddm_b200.shard import backward_sharded, gather_outputs
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    hg = H.HostGrid.adaptive(10, 1500, 8, seed=7)        # every rank builds the same grid
+    gold = O.Gold(*hg.arrays())
+    X = H.gen_points(10, 77, kind=2, seed=4, kink_reject=1e-6)
+    C = np.random.default_rng(5).standard_normal((len(X), 8))
+    lo, hi = shard_range(len(X), rank, world)
+
+    def oracle_backward(grid, x, gout):
+        gx, gs = grid.gradient(x.numpy(), gout.numpy())
+        return torch.from_numpy(gx), torch.from_numpy(gs)
+
+    gx, gs = backward_sharded(gold, torch.from_numpy(X[lo:hi]), torch.from_numpy(C[lo:hi]),
+                              backward=oracle_backward)
+    gx_all = gather_outputs(gx, len(X))
+    if rank == 0:
+        rx, rs = gold.gradient(X, C)
+        ret.put((bool(np.array_equal(gx_all.numpy(), rx)),
+                 float(np.abs(gs.numpy() - rs).max() / np.abs(rs).max())))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_gloo_sharded_backward():
+    """dL/dx stays per point; dL/dsurplus summed over both ranks' points by
+    one all-reduce equals the whole batch's gradient (up to the order of the
+    FP64 additions)."""
+    ctx = mp.get_context("spawn")
+    ret = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bwd_worker, args=(r, 2, port, ret)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    gx_equal, gs_rel = ret.get(timeout=10)
+    assert gx_equal
+    assert gs_rel <= 1e-13
