@@ -1241,7 +1241,7 @@ int chunk_rows_env() { return g_chunk_override.load(); }
 
 // FP32C variant of the direct entry points (plans time their own);
 // sgi_set_fp32c_variant (or SGI_FP32C_VARIANT at start-up) overrides.
-constexpr int DEFAULT_VARIANT = 0;
+constexpr int DEFAULT_VARIANT = 1;
 std::atomic<int> g_variant{[]() { const char* e = getenv("SGI_FP32C_VARIANT"); return e ? atoi(e) : DEFAULT_VARIANT; }()};
 
 uint32_t float_bits(float f)
@@ -1365,11 +1365,10 @@ int chunk_rows(const DeviceWork* W, const sgi_grid* g0, int precision, long long
 {
 	const int env = chunk_rows_env();
 	if (env >= 0) return env >= maxnno ? 0 : env;
-	// rows filling one L2 (FP64) or two (FP32C, whose big terms and
-	// dropped terms leave part of each chunk unread): the autotuner's choice
-	// on the d=59, 1M-node, TotalDof=256 workload
+	// rows filling half the L2 (the FP32 rows for FP32C): the autotuner's
+	// choice for both forms on the d=59, 1M-node, TotalDof=256 workload
 	const long long row = (long long)g0->ld * (precision == SGI_FP64 ? 8 : 4);
-	const long long rows = std::max(1024ll, (long long)W->l2_bytes * (precision == SGI_FP64 ? 1 : 2) / row);
+	const long long rows = std::max(1024ll, (long long)W->l2_bytes / 2 / row);
 	if (npts < 4096 || maxnno <= rows) return 0;
 	return (int)rows;
 }
@@ -1795,9 +1794,10 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 	const bool pinned = cudaPointerGetAttributes(&ax, x) == cudaSuccess && ax.type == cudaMemoryTypeHost &&
 		cudaPointerGetAttributes(&ao, out) == cudaSuccess && ao.type == cudaMemoryTypeHost;
 	cudaGetLastError();
-	// two halves: every sub-batch repeats all node-chunk launches, so more
-	// sub-batches buy overlap with launch tails
-	const int nsub = !pinned ? 1 : npts >= 128 * 1024 ? 2 : 1;
+	// sub-batches of about 128k points (at most 8): the first sub-batch's copy
+	// in and the last one's copy out are all that the kernels do not hide,
+	// while every sub-batch repeats all node-chunk launches
+	const int nsub = !pinned ? 1 : (int)std::min(8ll, std::max(1ll, npts / (128 * 1024)));
 	std::vector<long long> cut(nsub + 1);
 	for (int b = 0; b <= nsub; b++) cut[b] = npts * b / nsub;
 	std::vector<sgi_grid_t> sg;
@@ -2013,7 +2013,7 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		if (precision == SGI_FP32C && !grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k);
 	}
 	const sgi_grid* g0 = grids[0];
-	const int variant = 0;
+	const int variant = g_variant.load();   // the FP32C kernel sgi_interpolate runs
 	if (fwd_smem(precision, g0->dim, true) > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	// count the launches first: reject before launching anything
 	const int passes = (g0->TD + PASS - 1) / PASS;

@@ -215,7 +215,7 @@ int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* o
 
 /* Node-range chunking of the forward launches (process-wide).  A grid whose
  * surplus rows exceed the L2 is walked in chunks of consecutive nodes (rows
- * filling one L2 for FP64, two for FP32C), every point against one chunk per launch, the outputs
+ * filling half the L2: FP64 rows for FP64, FP32 rows for FP32C), every point against one chunk per launch, the outputs
  * carried between chunks in FP64 (the FP64 form keeps gold's order and bits).
  * rows < 0: automatic (the default; batches under 4096 points are not
  * chunked); 0: never chunk; > 0: chunks of `rows` nodes.  Returns the previous
@@ -231,7 +231,7 @@ int sgi_set_chunk_rows(int rows);
  * node windows; 3-5 are 0-2 with the node-window walk forced.  The variants
  * order the FP64 additions of big terms and of FP32 partial sums differently,
  * so their results may differ in the last bits (all within the FP32C
- * tolerance).  variant < 0 restores the default (0).  Returns the previous
+ * tolerance).  variant < 0 restores the default (1).  Returns the previous
  * setting, or a negative error code.  No reference counterpart. */
 int sgi_set_fp32c_variant(int variant);
 
