@@ -178,7 +178,10 @@ int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const long long* p
  * TotalDof, device), writes gx = dL/dx (npts x dim, device; may be NULL) and
  * gsurplus = dL/dsurplus (nno x TotalDof in file row order, device; may be
  * NULL; overwritten).  Weights are recomputed, never stored; dL/dsurplus is
- * reduced without atomics.  No reference counterpart. */
+ * reduced without atomics.  Its scratch (about 40 bytes per active
+ * (point, node) pair when gsurplus is requested) comes from a per-device
+ * memory pool that keeps freed memory for later calls until the process
+ * exits.  No reference counterpart. */
 int sgi_backward(sgi_grid_t g, long long npts, const double* x, const double* gout,
 	double* gx, double* gsurplus, void* stream);
 
