@@ -527,6 +527,43 @@ def run_c3(args):
                       "grad_norms": {"dx": float(gx.norm()), "dsurplus": float(gs.norm())}}))
 
 
+def run_errors(args):
+    """FP32C max / RMS relative error against the FP64 form (bit-identical to the
+    reference's gold path, as the GPU tests check) on every config's inputs:
+    C0 regular d=4 level 4, TotalDof 8, 1024 points; C1 regular d=16 level 5,
+    TotalDof 32, 65,536 points; C2 eight adaptive d=30 grids, TotalDof 64,
+    ragged batches; C3 adaptive d=59, 300k nodes, TotalDof 128, 32,768
+    points; C4 the benchmark workload."""
+    import torch
+    import hddm_b200 as H
+    dev = torch.device("cuda", 0)
+
+    def errs(grids, X, counts=None):
+        x = torch.from_numpy(X).to(dev)
+        o64 = H.interpolate(grids, x, counts=counts, precision=H.FP64)
+        o32 = H.interpolate(grids, x, counts=counts, precision=H.FP32C)
+        emax, erms = _rel_err(torch, o32, o64)
+        return {"points": len(X), "max_rel_err": emax, "rms_rel_err": erms}
+
+    res = {}
+    g0 = H.HostGrid.regular(4, 4, 8, seed=0)
+    res["C0"] = dict(nno=g0.nno, **errs(H.Grid(g0, flags=H.BUILD_FP32), H.gen_points(4, 1024, kind=0, seed=0)))
+    g1 = H.HostGrid.regular(16, 5, 32, seed=1)
+    res["C1"] = dict(nno=g1.nno, **errs(H.Grid(g1, flags=H.BUILD_FP32), H.gen_points(16, 65536, kind=0, seed=1)))
+    rng = np.random.Generator(np.random.PCG64(2))
+    nnos = np.exp(rng.uniform(np.log(20_000), np.log(200_000), 8)).astype(int)
+    counts = rng.integers(1, 100_001, 8)
+    grids = [H.Grid(H.HostGrid.adaptive(30, int(n), 64, seed=200 + k), flags=H.BUILD_FP32) for k, n in enumerate(nnos)]
+    res["C2"] = dict(nno=nnos.tolist(), **errs(grids, H.gen_points(30, int(counts.sum()), kind=0, seed=2), list(counts)))
+    del grids
+    g3 = H.HostGrid.adaptive(59, 300_000, 128, seed=3)
+    res["C3"] = dict(nno=g3.nno, **errs(H.Grid(g3, flags=H.BUILD_FP32),
+                                         H.gen_points(59, 32768, kind=0, seed=3, kink_reject=1e-6)))
+    hg, X, _ = make_workload()
+    res["C4"] = dict(nno=hg.nno, **errs(H.Grid(hg, flags=H.BUILD_FP32), X))
+    print(json.dumps({"fp32c_vs_gold_exact_fp64": res}))
+
+
 def run_multistate(args):
     """The reference's own call shape: one point per state across 16 states
     (d=59, TotalDof=118, 200k nodes each), per-call latency."""
@@ -567,7 +604,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "chunksweep", "variantsweep"],
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "chunksweep", "variantsweep", "errors"],
                     help="c4 (default) is the benchmark line; the others print their own measurements")
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--sweep-variants", default="0,1,2", help="variantsweep: FP32C variants")
@@ -586,6 +623,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "errors":
+        run_errors(args)
     elif args.workload == "c2":
         run_c2(args)
     elif args.workload == "c3":
