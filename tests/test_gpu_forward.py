@@ -270,12 +270,13 @@ def test_graph_plan_bit_exact_and_replayable(cuda, chunk_rows):
                 assert O.rel_error(got[sub], ref)[0] <= FP32C_TOL, k
 
 
-@pytest.mark.parametrize("variant", range(3))
+@pytest.mark.parametrize("variant", [0, 1, 2, 4])
 @pytest.mark.parametrize("td,rows", [(256, 0), (256, 1500), (128, 0), (300, 2000), (64, 0), (20, 0)])
 def test_fp32c_variants_within_tolerance(cuda, variant, td, rows):
     """Every FP32C kernel variant (E = 1, 2 and 4 output layouts, one and two
-    output passes, chunked or not) stays within the FP32C tolerance of gold,
-    and the FP64 form stays bit-exact under the same settings."""
+    output passes, chunked or not; 0-2 walk by descent, 4 forces the window
+    walk) stays within the FP32C tolerance of gold, and the FP64 form stays
+    bit-exact under the same settings."""
     h = H.HostGrid.adaptive(59, 6000, td, seed=60 + td)
     g = H.Grid(h, flags=H.BUILD_FP32)
     X = H.gen_points(59, 700, kind=2, seed=61)
@@ -335,3 +336,47 @@ def test_host_entry_pipelined_sub_batches(cuda):
                 assert np.array_equal(dev[sl], O.Gold(*hosts[k].arrays()).interpolate(X[sl]))
         else:
             assert O.rel_error(outh.numpy(), dev)[0] <= 1e-9
+
+
+def _deep_chain_grid(dim, depth, td, seed):
+    """Nodes c_0 .. c_{depth-1}: c_k has the level-2 half hat at 0 (i=2, j=0)
+    in dimensions 0 .. k-1, so each holds the next (a chain of containment);
+    beside each c_k (k >= 1) a sibling with the half hat at 1 (i=2, j=2) in
+    dimension k-1 forms a pair with it.  Depth-first order: the chain, then the
+    siblings from the deepest up."""
+    rows = []
+    for k in range(depth):
+        r = np.zeros(2 * dim, np.int32)
+        r[:k] = 2
+        rows.append(r)
+    for k in range(depth - 1, 0, -1):
+        r = np.zeros(2 * dim, np.int32)
+        r[:k] = 2
+        r[dim + k - 1] = 2
+        rows.append(r)
+    idx = np.array(rows)
+    lev = np.where(idx[:, :dim] > 0, 1, 0).sum(axis=1)
+    sur = np.random.default_rng(seed).uniform(-1, 1, (len(idx), td)) * 4.0 ** (-lev[:, None])
+    return idx, sur
+
+
+@pytest.mark.parametrize("rows", [0, 7])
+def test_deep_tree_descent_and_fallback(cuda, rows):
+    """A containment tree of depth 46: the FP32C descent handles it whole
+    (depth <= 64); in node chunks (chains must be complete, depth <= 32) the
+    window walk takes over.  FP64 bit-exact, FP32C within tolerance."""
+    dim, depth = 48, 46
+    idx, sur = _deep_chain_grid(dim, depth, 64, seed=3)
+    hg = H.HostGrid.from_dense(idx, sur)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    assert g.info.tree_depth == depth
+    rng = np.random.default_rng(4)
+    X = rng.uniform(0.0, 0.5, (400, dim))          # deep in the chain ...
+    X[::3, rng.integers(0, dim, 400)[::3]] = 0.75  # ... and points that leave it early
+    ref = O.Gold(idx, sur).interpolate(X)
+    prev = H.set_chunk_rows(rows)
+    try:
+        assert np.array_equal(_run(g, X), ref)
+        assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
+    finally:
+        H.set_chunk_rows(prev)
