@@ -75,3 +75,20 @@ def test_load_checks_nagents_and_state_range(tmp_path):
     (tmp_path / "hddm-solver.cfg").write_text("priorityCUDA 2\nn_agents 59\n")
     r = _run(f"d = lib.getData(1); lib.sgi_plugin_data_load(d, {plt!r}.encode(), 3)", tmp_path)
     assert r.returncode != 0 and "State 3 index out of range 0 .. 0" in r.stderr
+
+
+def _build_plugin_host(out_dir):
+    """Compiles tests/plugin_host.cpp, the parent-loader stand-in (dlopen +
+    dlsym + virtual calls through include/sgi_plugin.h); returns its path."""
+    root = os.path.dirname(PKG)
+    exe = os.path.join(str(out_dir), "plugin_host")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "plugin_host.cpp"), "-o", exe, "-ldl"],
+                   check=True, capture_output=True, text=True)
+    return exe
+
+
+def test_plugin_host_compiles_against_the_plugin_header(tmp_path):
+    """The reference-side binding a maintainer adds compiles against the
+    plugin header alone (no link against the library)."""
+    assert os.path.exists(_build_plugin_host(tmp_path))
