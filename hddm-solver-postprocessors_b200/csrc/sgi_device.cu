@@ -6,8 +6,11 @@
 // Every node's support lies inside its tree parent's support, and a node's
 // subtree is the index range [n, skip[n]).
 //
-// Forward kernel: one warp per query point, points pulled from a device work
-// counter.  The warp walks the nodes in windows of 32 consecutive indices:
+// Forward kernels: one warp per query point, points pulled from a device work
+// counter.  Two walks find a point's active nodes.
+//
+// Window walk (FP64 form, hit counts, backward, FP32C fallback): the warp
+// walks the nodes in windows of 32 consecutive indices:
 //   * lane k checks node n0+k against the point with one hat evaluation (the
 //     component in which it differs from its parent);
 //   * an inclusive max-scan of the skip pointers of failing nodes marks every
@@ -22,6 +25,13 @@
 // operations in its order (LinearBasis/gold/src/InterpolateArray.cpp:26-41):
 // the same multiplies for the weight and the same multiply-then-add sequence per
 // output, so its results are bit-identical to gold's.
+//
+// Descent walk (FP32C form, fwd_f32d_kernel): the warp keeps a stack of child
+// groups of active nodes (left/right child pairs per dimension, see
+// sgi::build_descent) and evaluates one group per lane, 32 per step; a hit's
+// weight is its parent's times its hat over the parent's hat in that
+// dimension, and terms are split by size into FP64 rows (big), FP32 rows
+// (fine) and dropped ones (negligible).
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
@@ -62,7 +72,7 @@ struct GridDesc
 	const uint4* ninfo;          //   per node: {first group, group count, rowmax bits, FP64 copy row or NONE}
 	int depth;                   // containment-tree depth (bounds the descent stack)
 	float skip_below;            // FP32C drops fine terms with |w| * rowmax below this
-	float big_below;             // FP32C list form: terms with |w| * rowmax from this up are big
+	float big_below;             // FP32C: terms with |w| * rowmax from this up are big (FP64 rows)
 	long long pt_begin;
 	int nno;
 	int ld;
