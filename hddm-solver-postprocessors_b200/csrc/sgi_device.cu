@@ -1879,10 +1879,12 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 	const bool pinned = cudaPointerGetAttributes(&ax, x) == cudaSuccess && ax.type == cudaMemoryTypeHost &&
 		cudaPointerGetAttributes(&ao, out) == cudaSuccess && ao.type == cudaMemoryTypeHost;
 	cudaGetLastError();
-	// sub-batches of about 128k points (at most 8): the first sub-batch's copy
+	// sub-batches of about 256k points (at most 8): the first sub-batch's copy
 	// in and the last one's copy out are all that the kernels do not hide,
-	// while every sub-batch repeats all node-chunk launches
-	const int nsub = !pinned ? 1 : (int)std::min(8ll, std::max(1ll, npts / (128 * 1024)));
+	// while every sub-batch repeats all node-chunk launches and their tails
+	// (on d=59, 1M nodes, TotalDof 256, 1M points: 1, 2, 4, 8, 16 sub-batches
+	// took 147, 129, 125, 131, 155 ms)
+	const int nsub = !pinned ? 1 : (int)std::min(8ll, std::max(1ll, npts / (256 * 1024)));
 	std::vector<long long> cut(nsub + 1);
 	for (int b = 0; b <= nsub; b++) cut[b] = npts * b / nsub;
 	std::vector<sgi_grid_t> sg;

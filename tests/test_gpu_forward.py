@@ -313,13 +313,14 @@ def test_wide_component_form_bit_exact(cuda):
 
 
 def test_host_entry_pipelined_sub_batches(cuda):
-    """Pinned host buffers with >= 128k points go through overlapped
-    copy-in / kernel / copy-out sub-batches; FP64 stays gold-exact."""
+    """Pinned host buffers with >= 512k points go through overlapped
+    copy-in / kernel / copy-out sub-batches (here two, the cut inside the
+    first grid's points); FP64 stays gold-exact."""
     import ctypes
     import torch
     hosts = [H.HostGrid.adaptive(8, 3000, 40, seed=60), H.HostGrid.adaptive(8, 1500, 40, seed=61)]
     grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
-    counts = [150_000, 60_000]
+    counts = [450_000, 150_000]
     X = H.gen_points(8, sum(counts), kind=2, seed=62)
     xh = torch.from_numpy(X).pin_memory()
     outh = torch.zeros((sum(counts), 40), dtype=torch.float64).pin_memory()
@@ -331,8 +332,8 @@ def test_host_entry_pipelined_sub_batches(cuda):
         dev = _run(grids, X, precision, counts=counts)
         if precision == H.FP64:
             assert np.array_equal(outh.numpy(), dev)
-            sub = np.r_[0:150_000:997, 150_000:210_000:499]
-            for k, sl in ((0, sub[sub < 150_000]), (1, sub[sub >= 150_000])):
+            sub = np.r_[0:450_000:1997, 450_000:600_000:997]
+            for k, sl in ((0, sub[sub < 450_000]), (1, sub[sub >= 450_000])):
                 assert np.array_equal(dev[sl], O.Gold(*hosts[k].arrays()).interpolate(X[sl]))
         else:
             assert O.rel_error(outh.numpy(), dev)[0] <= 1e-9
