@@ -529,7 +529,8 @@ def run_c3(args):
 
 def run_errors(args):
     """FP32C max / RMS relative error against the FP64 form (bit-identical to the
-    reference's gold path, as the GPU tests check) on every config's inputs:
+    reference's gold path, as the GPU tests check), and both forms' step times
+    (graph-plan replays), on every config's inputs:
     C0 regular d=4 level 4, TotalDof 8, 1024 points; C1 regular d=16 level 5,
     TotalDof 32, 65,536 points; C2 eight adaptive d=30 grids, TotalDof 64,
     ragged batches; C3 adaptive d=59, 300k nodes, TotalDof 128, 32,768
@@ -538,12 +539,20 @@ def run_errors(args):
     import hddm_b200 as H
     dev = torch.device("cuda", 0)
 
+    stream = torch.cuda.current_stream(dev)
+
     def errs(grids, X, counts=None):
         x = torch.from_numpy(X).to(dev)
         o64 = H.interpolate(grids, x, counts=counts, precision=H.FP64)
         o32 = H.interpolate(grids, x, counts=counts, precision=H.FP32C)
         emax, erms = _rel_err(torch, o32, o64)
-        return {"points": len(X), "max_rel_err": emax, "rms_rel_err": erms}
+        # step times of autotuned graph plans of both forms (CUDA events)
+        p64 = H.Plan(grids, x, o64, counts=counts, precision=H.FP64, stream=stream)
+        p32 = H.Plan(grids, x, o32, counts=counts, precision=H.FP32C, stream=stream)
+        ms64 = _plan_time(H, torch, p64, stream, max(args.steps, 5), args.warmup)
+        ms32 = _plan_time(H, torch, p32, stream, max(args.steps, 5), args.warmup)
+        return {"points": len(X), "max_rel_err": emax, "rms_rel_err": erms,
+                "fp64_ms": ms64, "fp32c_ms": ms32, "fp32c_points_per_s": len(X) / ms32 * 1e3}
 
     res = {}
     g0 = H.HostGrid.regular(4, 4, 8, seed=0)

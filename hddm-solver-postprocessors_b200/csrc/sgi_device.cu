@@ -2276,15 +2276,15 @@ extern "C" int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long l
 		}
 		if (!hit)
 		{
-			// candidates: no chunks, and chunks whose rows fill 1/4 .. 2 x the
-			// L2 (or the requested chunk); kernel variants for FP32C
+			// candidates: no chunks, and chunks whose rows fill 1/4, 1/2, 3/4, 1
+			// and 2 L2s (or the requested chunk); kernel variants for FP32C
 			std::vector<int> cand;
 			if (chunk >= 0) cand.push_back(chunk);
 			else
 			{
 				const long long row = (long long)grids[0]->ld * (precision == SGI_FP64 ? 8 : 4);
 				cand.push_back(0);
-				for (double f : { 0.25, 0.5, 1.0, 2.0 })
+				for (double f : { 0.25, 0.5, 0.75, 1.0, 2.0 })
 				{
 					const long long r = std::max(1024ll, (long long)(W->l2_bytes * f / row));
 					if (r < maxnno) cand.push_back((int)r);

@@ -247,7 +247,7 @@ int sgi_set_fp32c_variant(int variant);
  * chunk_rows >= 0 fixes the node-chunk size (0 = none); chunk_rows < 0 lets the
  * autotuner choose it: the first time a (dim, largest nno, TotalDof,
  * precision, point count) key is seen, candidate chunk sizes (none, and rows
- * filling 1/4, 1/2, 1 and 2 L2s), and for FP32C the kernel variants, are timed
+ * filling 1/4, 1/2, 3/4, 1 and 2 L2s), and for FP32C the kernel variants, are timed
  * on the given inputs (which runs the forward, overwriting out) and the
  * fastest is cached for the process.
  * Replays of one plan must not overlap each other.  No reference counterpart
