@@ -436,7 +436,11 @@ __device__ __forceinline__ void load_row(const float* row, int o, bool in, float
 	else d[0] = in ? __ldg(row + o) : 0.f;
 }
 
-template <int V, int E>
+// QH: rows in flight per warp.  A window's hits are taken QH at a time in
+// index order: their rows are all loaded before the first is added, and the
+// adds follow the gold order.  Two rows suit large batches (registers buy
+// warps); small batches, whose few warps wait on each row, use more.
+template <int V, int E, int QH = 2>
 __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ FwdArgs a)
 {
 	extern __shared__ double smem[];
@@ -478,36 +482,39 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_kernel(const __grid_constant__ 
 		{
 			traverse<false>(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&, float)
 			{
-				// two hits per step, both rows loaded before either is added, so
-				// that each warp keeps two rows in flight; the adds stay in order
+				// QH hits per step, all their rows loaded before any is added, so
+				// that each warp keeps QH rows in flight; the adds stay in order
 				while (mask)
 				{
-					const int k0 = __ffs(mask) - 1;
-					mask &= mask - 1;
-					const bool two = mask != 0u;
-					const int k1 = two ? __ffs(mask) - 1 : k0;
-					if (two) mask &= mask - 1;
-					const double w0 = __shfl_sync(FULL, w, k0);
-					const double w1 = __shfl_sync(FULL, w, k1);
-					const double* row0 = G.s64 + (size_t)(n0 + k0) * G.ld + a.o_begin;
-					const double* row1 = G.s64 + (size_t)(n0 + k1) * G.ld + a.o_begin;
-					double s0[V][E], s1[V][E];
+					int kq[QH];
 #pragma unroll
-					for (int v = 0; v < V; v++)
+					for (int q = 0; q < QH; q++)
 					{
-						const int o = out_col<E>(v, lane);
-						const bool in = a.o_begin + o < G.ld;
-						load_row<E>(row0, o, in, s0[v]);
-						load_row<E>(row1, o, in && two, s1[v]);
+						kq[q] = mask ? __ffs(mask) - 1 : -1;
+						if (mask) mask &= mask - 1;
+					}
+					double sq[QH][V][E];
+#pragma unroll
+					for (int q = 0; q < QH; q++)
+					{
+						const double* row = G.s64 + (size_t)(n0 + (kq[q] >= 0 ? kq[q] : kq[0])) * G.ld + a.o_begin;
+#pragma unroll
+						for (int v = 0; v < V; v++)
+						{
+							const int o = out_col<E>(v, lane);
+							load_row<E>(row, o, kq[q] >= 0 && a.o_begin + o < G.ld, sq[q][v]);
+						}
 					}
 #pragma unroll
-					for (int v = 0; v < V; v++)
+					for (int q = 0; q < QH; q++)
+					{
+						if (kq[q] < 0) break;   // warp-uniform
+						const double wq = __shfl_sync(FULL, w, kq[q]);
 #pragma unroll
-						for (int e = 0; e < E; e++)
-						{
-							acc[v][e] = __dadd_rn(acc[v][e], __dmul_rn(w0, s0[v][e]));
-							if (two) acc[v][e] = __dadd_rn(acc[v][e], __dmul_rn(w1, s1[v][e]));
-						}
+						for (int v = 0; v < V; v++)
+#pragma unroll
+							for (int e = 0; e < E; e++) acc[v][e] = __dadd_rn(acc[v][e], __dmul_rn(wq, sq[q][v][e]));
+					}
 				}
 			}, nullptr, pathmask, a.chain_len[gi]);
 		}
@@ -1373,17 +1380,21 @@ void (*fp32c_kernel(int variant, bool descent, int cols))(FwdArgs)
 	return cols == V * 32 * E ? f32d_variant<V, E, true>(variant) : f32d_variant<V, E, false>(variant);
 }
 
-void (*select_fwd(int precision, int ld, int cols, int variant = 0, bool descent = false))(FwdArgs)
+// small: a batch of fewer points than resident warps; the FP64 form then
+// keeps eight rows in flight per warp (four for eight outputs per lane).
+void (*select_fwd(int precision, int ld, int cols, int variant = 0, bool descent = false, bool small = false))(FwdArgs)
 {
 	const bool f64 = precision == SGI_FP64;
-	if (ld <= 32) return f64 ? fwd_f64_kernel<1, 1> : fp32c_kernel<1, 1>(variant, descent, cols);
-	if (cols <= 64) return f64 ? fwd_f64_kernel<1, 2> : fp32c_kernel<1, 2>(variant, descent, cols);
+	if (ld <= 32) return f64 ? (small ? fwd_f64_kernel<1, 1, 8> : fwd_f64_kernel<1, 1>) : fp32c_kernel<1, 1>(variant, descent, cols);
+	if (cols <= 64) return f64 ? (small ? fwd_f64_kernel<1, 2, 8> : fwd_f64_kernel<1, 2>) : fp32c_kernel<1, 2>(variant, descent, cols);
 	// FP32C reads four consecutive outputs per lane (16-byte loads) when rows
 	// are a multiple of 128 wide
 	const bool e4 = !f64 && ld % 128 == 0;
 	if (cols <= 128)
-		return f64 ? fwd_f64_kernel<2, 2> : e4 ? fp32c_kernel<1, 4>(variant, descent, cols) : fp32c_kernel<2, 2>(variant, descent, cols);
-	return f64 ? fwd_f64_kernel<4, 2> : e4 ? fp32c_kernel<2, 4>(variant, descent, cols) : fp32c_kernel<4, 2>(variant, descent, cols);
+		return f64 ? (small ? fwd_f64_kernel<2, 2, 8> : fwd_f64_kernel<2, 2>)
+		           : e4 ? fp32c_kernel<1, 4>(variant, descent, cols) : fp32c_kernel<2, 2>(variant, descent, cols);
+	return f64 ? (small ? fwd_f64_kernel<4, 2, 4> : fwd_f64_kernel<4, 2>)
+	           : e4 ? fp32c_kernel<2, 4>(variant, descent, cols) : fp32c_kernel<4, 2>(variant, descent, cols);
 }
 
 // Dynamic shared memory of a forward launch.
@@ -1792,7 +1803,8 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 			set_starts(a, grids, gb, ng);
 			a.counter = counters ? counters + launches : W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant, descent);
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant, descent,
+				a.npts < (long long)W->sms * WARPS);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, W->sms, &blocks);
@@ -2154,7 +2166,8 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 			a.o_begin = ob;
 			a.counter = counters + slot++;
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant, descent);
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant, descent,
+				a.npts < (long long)sms * WARPS);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, sms, &blocks);
