@@ -1331,10 +1331,21 @@ std::atomic<int> g_chunk_override{[]() { const char* e = getenv("SGI_CHUNK_ROWS"
 
 int chunk_rows_env() { return g_chunk_override.load(); }
 
-// FP32C variant of the direct entry points (plans time their own);
-// sgi_set_fp32c_variant (or SGI_FP32C_VARIANT at start-up) overrides.
-constexpr int DEFAULT_VARIANT = 1;
-std::atomic<int> g_variant{[]() { const char* e = getenv("SGI_FP32C_VARIANT"); return e ? atoi(e) : DEFAULT_VARIANT; }()};
+// FP32C variant of the direct entry points (plans time their own): -1 =
+// automatic (auto_variant), else the variant sgi_set_fp32c_variant (or
+// SGI_FP32C_VARIANT at start-up) fixed.
+std::atomic<int> g_variant{[]() { const char* e = getenv("SGI_FP32C_VARIANT"); return e ? atoi(e) : -1; }()};
+
+// The automatic FP32C variant: eight fine rows in flight per warp (2) for a
+// batch of fewer than 64 points per SM, whose warps wait on their rows (on a
+// 200k-node d=59 grid, 16 / 1,024 / 8,192 points: 242 / 451 / 994 us against
+// 327 / 661 / 1,130 us for variant 1), else two rows at 4 blocks per SM (1),
+// the faster at a million points.
+int auto_variant(int variant, long long npts, int sms)
+{
+	if (variant >= 0) return variant;
+	return npts < (long long)sms * 64 ? 2 : 1;
+}
 
 uint32_t float_bits(float f)
 {
@@ -1651,8 +1662,10 @@ extern "C" int sgi_set_chunk_rows(int rows)
 extern "C" int sgi_set_fp32c_variant(int variant)
 {
 	clear_error();
-	if (variant >= NVARIANTS_ALL) return fail(SGI_E_INVALID, "FP32C variant %d out of range (0..%d)", variant, NVARIANTS_ALL - 1);
-	return g_variant.exchange(variant < 0 ? DEFAULT_VARIANT : variant);
+	if (variant >= NVARIANTS_ALL && variant != SGI_FP32C_AUTO)
+		return fail(SGI_E_INVALID, "FP32C variant %d out of range (0..%d, or SGI_FP32C_AUTO)", variant, NVARIANTS_ALL - 1);
+	const int prev = g_variant.exchange(variant < 0 || variant == SGI_FP32C_AUTO ? -1 : variant);
+	return prev < 0 ? SGI_FP32C_AUTO : prev;
 }
 
 extern "C" int sgi_last_launch(sgi_launch_stats* s)
@@ -1763,7 +1776,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 	double* out, int precision, cudaStream_t stream, int chunk = -1, unsigned long long* counters = nullptr,
 	int* nlaunch = nullptr, int variant = -1)
 {
-	if (variant < 0) variant = g_variant.load();
+	if (variant < 0) variant = g_variant.load();   // may stay -1: automatic per launch group
 	const sgi_grid* g0 = grids[0];
 	DeviceWork* W = nullptr;
 	int rc = device_work(g0->device, &W);
@@ -1803,8 +1816,8 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 			set_starts(a, grids, gb, ng);
 			a.counter = counters ? counters + launches : W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant, descent,
-				a.npts < (long long)W->sms * WARPS);
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS),
+				auto_variant(variant, a.npts, W->sms), descent, a.npts < (long long)W->sms * WARPS);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, W->sms, &blocks);
@@ -2127,7 +2140,7 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		if (precision == SGI_FP32C && !grids[k]->s32) return fail(SGI_E_INVALID, "grid %d was built without SGI_BUILD_FP32", k);
 	}
 	const sgi_grid* g0 = grids[0];
-	const int variant = g_variant.load();   // the FP32C kernel sgi_interpolate runs
+	const int variant = g_variant.load();   // resolved per group as sgi_interpolate does
 	if (fwd_smem(precision, g0->dim, true) > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	// count the launches first: reject before launching anything
 	const int passes = (g0->TD + PASS - 1) / PASS;
@@ -2166,8 +2179,8 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 			a.o_begin = ob;
 			a.counter = counters + slot++;
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS), variant, descent,
-				a.npts < (long long)sms * WARPS);
+			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS),
+				auto_variant(variant, a.npts, sms), descent, a.npts < (long long)sms * WARPS);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, sms, &blocks);

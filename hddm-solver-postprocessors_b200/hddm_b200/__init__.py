@@ -365,9 +365,13 @@ def set_chunk_rows(rows):
     return lib.sgi_set_chunk_rows(rows)
 
 
+FP32C_AUTO = 255
+
+
 def set_fp32c_variant(variant):
-    """FP32C kernel variant of interpolate/interpolate_host (-1: default);
-    returns the previous one."""
+    """FP32C kernel variant of interpolate/interpolate_host (-1 or FP32C_AUTO:
+    automatic by batch size); returns the previous one (FP32C_AUTO when
+    automatic), which restores it when passed back."""
     rc = lib.sgi_set_fp32c_variant(variant)
     if rc < 0:
         _check(rc)

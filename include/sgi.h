@@ -234,8 +234,12 @@ int sgi_set_chunk_rows(int rows);
  * node windows; 3-5 are 0-2 with the node-window walk forced.  The variants
  * order the FP64 additions of big terms and of FP32 partial sums differently,
  * so their results may differ in the last bits (all within the FP32C
- * tolerance).  variant < 0 restores the default (1).  Returns the previous
- * setting, or a negative error code.  No reference counterpart. */
+ * tolerance).  variant < 0 or SGI_FP32C_AUTO restores the default,
+ * automatic: 2 for a launch with fewer than 64 points per SM (9,472 on a
+ * B200), else 1.  Returns the previous setting
+ * (SGI_FP32C_AUTO for automatic), or a negative error code.  No reference
+ * counterpart. */
+#define SGI_FP32C_AUTO 255
 int sgi_set_fp32c_variant(int variant);
 
 /* Plans: one forward call recorded into a CUDA graph and replayed.
