@@ -1034,6 +1034,88 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 	}
 }
 
+// Small batches of the FP64 form (fewer points than resident warps, not
+// node-chunked): one warp per (point, block of 32 outputs of the pass), lane
+// l owning output 32 * block + l.  Each warp walks the tree itself (the
+// blocks of one point walk in parallel) and lists its hits, with their
+// gold-order weights, in index order in shared memory; the list is drained
+// CDEPTH rows at a time, every lane loading its output of CDEPTH rows before
+// the adds, which follow the gold order.  One double per lane per row lets a
+// warp keep CDEPTH rows in flight where fwd_f64_kernel, owning up to eight
+// outputs per lane, keeps eight.
+constexpr int CLIST = 64;
+constexpr int CDEPTH = 16;
+
+__host__ __device__ __forceinline__ int cols_stride(int dim) { return CLIST + CLIST / 2 + ((dim + 1) & ~1); }
+
+__global__ void __launch_bounds__(BLOCK) fwd_f64_cols_kernel(const __grid_constant__ FwdArgs a)
+{
+	extern __shared__ double smem[];
+	const int lane = threadIdx.x & 31;
+	double* wbase = smem + (threadIdx.x >> 5) * cols_stride(a.dim);
+	double* lw = wbase;
+	uint32_t* ln = reinterpret_cast<uint32_t*>(wbase + CLIST);
+	double* xs = wbase + CLIST + CLIST / 2;
+	const int cols = min(a.TD - a.o_begin, PASS);
+	const int ncb = (cols + 31) / 32;
+	const long long nitems = a.npts * ncb;
+	for (;;)
+	{
+		long long it = 0;
+		if (lane == 0) it = (long long)atomicAdd(a.counter, 1ull);
+		it = __shfl_sync(FULL, it, 0);
+		if (it >= nitems) break;
+		const long long p = it / ncb;
+		const int col = (int)(it % ncb) * 32 + lane;
+		const bool cin = col < cols;
+		const GridDesc& G = a.g[find_grid(a, p)];
+		const bool ok = load_point(a, p, xs, lane);
+		double acc = 0.0;
+		int n = 0;
+		// list entries [0, cnt) in order
+		auto drain = [&](int cnt)
+		{
+			for (int b = 0; b < cnt; b += CDEPTH)
+			{
+				double sv[CDEPTH];
+#pragma unroll
+				for (int q = 0; q < CDEPTH; q++)
+					sv[q] = (b + q < cnt && cin) ? __ldg(G.s64 + (size_t)ln[b + q] * G.ld + a.o_begin + col) : 0.0;
+#pragma unroll
+				for (int q = 0; q < CDEPTH; q++)
+				{
+					if (b + q >= cnt) break;   // warp-uniform
+					acc = __dadd_rn(acc, __dmul_rn(lw[b + q], sv[q]));
+				}
+			}
+		};
+		if (ok)
+		{
+			traverse<false>(G, xs, lane, 0, G.nno, [&](unsigned mask, int n0, double w, const uint4&, float)
+			{
+				if ((mask >> lane) & 1u)
+				{
+					const int pos = n + __popc(mask & ((1u << lane) - 1u));
+					ln[pos] = (uint32_t)(n0 + lane);
+					lw[pos] = w;
+				}
+				n += __popc(mask);   // below 32 before, below CLIST after
+				__syncwarp();
+				if (n >= 32)
+				{
+					drain(n);
+					n = 0;
+					__syncwarp();
+				}
+			});
+			if (n) drain(n);
+		}
+		if (cin)
+			a.out[(size_t)p * a.TD + a.o_begin + col] = ok ? acc : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0);
+		__syncwarp();
+	}
+}
+
 // Active-node count per point (single grid).
 __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ FwdArgs a, long long* counts)
 {
@@ -1806,7 +1888,11 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 		const int clen = chunk < 0 ? chunk_rows(W, g0, precision, a.npts, maxnno) : (chunk >= maxnno ? 0 : chunk);
 		const int nchunks = clen ? (maxnno + clen - 1) / clen : 1;
 		const bool descent = precision == SGI_FP32C && descent_ok(grids, gb, ng, clen > 0);
-		const size_t smem = fwd_smem(precision, g0->dim, descent);
+		const bool small = a.npts < (long long)W->sms * WARPS;
+		// small unchunked FP64 batches: one warp per (point, 32 outputs)
+		const bool cols_mode = precision == SGI_FP64 && small && clen == 0;
+		const size_t smem = cols_mode ? (size_t)WARPS * cols_stride(g0->dim) * sizeof(double)
+		                              : fwd_smem(precision, g0->dim, descent);
 		for (int ob = 0; ob < g0->TD; ob += PASS)
 		for (int c = 0; c < std::max(nchunks, 1); c++)
 		{
@@ -1816,13 +1902,15 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 			set_starts(a, grids, gb, ng);
 			a.counter = counters ? counters + launches : W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS),
-				auto_variant(variant, a.npts, W->sms), descent, a.npts < (long long)W->sms * WARPS);
+			const int cols = std::min(g0->TD - ob, PASS);
+			void (*kern)(FwdArgs) = cols_mode ? fwd_f64_cols_kernel
+				: select_fwd(precision, g0->ld, cols, auto_variant(variant, a.npts, W->sms), descent, small);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, W->sms, &blocks);
 			if (rc) return rc;
-			const long long need = (a.npts + WARPS - 1) / WARPS;
+			const long long items = cols_mode ? a.npts * ((cols + 31) / 32) : a.npts;
+			const long long need = (items + WARPS - 1) / WARPS;
 			if (blocks > need) blocks = (int)need;
 			kern<<<blocks, BLOCK, smem, stream>>>(a);
 			CUDA_TRY(cudaGetLastError());
