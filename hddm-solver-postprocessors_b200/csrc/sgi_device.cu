@@ -2260,20 +2260,26 @@ extern "C" int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, cons
 		a.npts = p1 - p0;
 		a.ngrids = ng; a.dim = g0->dim; a.TD = g0->TD;
 		set_starts(a, grids, gb, ng);   // whole grids: the roots' groups
+		// the kernels sgi_interpolate picks for an unchunked launch
 		const bool descent = precision == SGI_FP32C && descent_ok(grids, gb, ng, false);
-		const size_t smem = fwd_smem(precision, g0->dim, descent);
+		const bool small = a.npts < (long long)sms * WARPS;
+		const bool cols_mode = precision == SGI_FP64 && small;
+		const size_t smem = cols_mode ? (size_t)WARPS * cols_stride(g0->dim) * sizeof(double)
+		                              : fwd_smem(precision, g0->dim, descent);
 		for (int ob = 0; ob < g0->TD; ob += PASS)
 		{
 			a.o_begin = ob;
 			a.counter = counters + slot++;
 			CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream));
-			void (*kern)(FwdArgs) = select_fwd(precision, g0->ld, std::min(g0->TD - ob, PASS),
-				auto_variant(variant, a.npts, sms), descent, a.npts < (long long)sms * WARPS);
+			const int cols = std::min(g0->TD - ob, PASS);
+			void (*kern)(FwdArgs) = cols_mode ? fwd_f64_cols_kernel
+				: select_fwd(precision, g0->ld, cols, auto_variant(variant, a.npts, sms), descent, small);
 			if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			int blocks = 0;
 			rc = occupancy_grid(kern, smem, sms, &blocks);
 			if (rc) return rc;
-			const long long need = (a.npts + WARPS - 1) / WARPS;
+			const long long items = cols_mode ? a.npts * ((cols + 31) / 32) : a.npts;
+			const long long need = (items + WARPS - 1) / WARPS;
 			if (blocks > need) blocks = (int)need;
 			kern<<<blocks, BLOCK, smem, stream>>>(a);
 			CUDA_TRY(cudaGetLastError());

@@ -37,11 +37,13 @@ def _noalloc(grids, x, counts, precision, out):
     return _fn(len(grids), arr, offs.ctypes.data, x.data_ptr(), out.data_ptr(), precision, stream)
 
 
-def test_noalloc_matches_allocating_entry_point(cuda):
+@pytest.mark.parametrize("counts", [[700, 0, 13, 1500], [5, 0, 3, 9]])
+def test_noalloc_matches_allocating_entry_point(cuda, counts):
+    """A batch of 2,213 points, and one of 17 (small batches take their own
+    kernels), through both entry points."""
     import torch
     hosts = [H.HostGrid.adaptive(30, n, 300, seed=40 + k) for k, n in enumerate((3000, 9000, 500, 6000))]
     grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
-    counts = [700, 0, 13, 1500]
     X = H.gen_points(30, sum(counts), kind=2, seed=12)
     x = torch.from_numpy(X).cuda()
     ref64 = H.interpolate(grids, x, counts=counts, precision=H.FP64).cpu().numpy()
