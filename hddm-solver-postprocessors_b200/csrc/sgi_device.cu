@@ -1995,11 +1995,23 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 	// sub-batches of about 256k points (at most 8): the first sub-batch's copy
 	// in and the last one's copy out are all that the kernels do not hide,
 	// while every sub-batch repeats all node-chunk launches and their tails
-	// (on d=59, 1M nodes, TotalDof 256, 1M points: 1, 2, 4, 8, 16 sub-batches
-	// took 147, 129, 125, 131, 155 ms)
-	const int nsub = !pinned ? 1 : (int)std::min(8ll, std::max(1ll, npts / (256 * 1024)));
+	// (on d=59, 1M nodes, TotalDof 256, 1M points: 1, 2, 4, 8, 16 equal
+	// sub-batches took 147, 129, 125, 131, 155 ms).  With three or more, the
+	// first and the last are half the size of the others: their exposed
+	// copies shrink while each middle sub-batch's copy out still fits under
+	// the next one's kernels.
+	const int nsub = !pinned ? 1 : (int)std::min(8ll, std::max(1ll, (npts + 128 * 1024) / (256 * 1024)));
 	std::vector<long long> cut(nsub + 1);
-	for (int b = 0; b <= nsub; b++) cut[b] = npts * b / nsub;
+	{
+		const long long units = nsub >= 3 ? 2ll * nsub - 2 : nsub;   // weights 1, 2, ..., 2, 1
+		long long acc = 0;
+		cut[0] = 0;
+		for (int b = 0; b < nsub; b++)
+		{
+			acc += (nsub >= 3 && b > 0 && b < nsub - 1) ? 2 : 1;
+			cut[b + 1] = npts * acc / units;
+		}
+	}
 	std::vector<sgi_grid_t> sg;
 	std::vector<long long> so;
 	for (int b = 0; b < nsub; b++)
