@@ -607,17 +607,47 @@ def run_multistate(args):
                                                           "large, avx2 (daint)": 4.234e-3}}))
 
 
+def run_cutoffsweep(args):
+    """FP32C step time (graph replay) and error against the gold-exact FP64 form
+    for surplus cutoffs of 2^-k of the largest |surplus|, default workload."""
+    import torch
+    import hddm_b200 as H
+    dev = torch.device("cuda", 0)
+    hg, X, _ = make_workload(npts=args.points)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    x = torch.from_numpy(X).to(dev)
+    ref = H.interpolate(g, x, precision=H.FP64)
+    smax = g.set_surplus_cutoff(0.0) * 2.0 ** 46
+    stream = torch.cuda.Stream(dev)
+    res = []
+    for k in [int(v) for v in args.sweep_cutoffs.split(",")]:
+        eff = g.set_surplus_cutoff(smax * 2.0 ** -k)
+        out = torch.empty(x.shape[0], TD, dtype=torch.float64, device=dev)
+        plan = H.Plan(g, x, out, precision=H.FP32C, chunk_rows=args.chunk_rows, stream=stream)
+        ms = _plan_time(H, torch, plan, stream, 5, 3)
+        emax, erms = _rel_err(torch, out, ref)
+        res.append({"cutoff_log2_of_max_surplus": -k, "cutoff": eff, "ms": ms, "max_rel_err": emax,
+                    "rms_rel_err": erms, "chunk_rows": plan.chunk_rows, "variant": plan.variant})
+        print(json.dumps(res[-1]), file=sys.stderr)
+        del plan
+    g.set_surplus_cutoff(0.0)
+    print(json.dumps({"workload": WORKLOAD, "cutoff_sweep": res}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "chunksweep", "variantsweep", "errors"],
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "chunksweep", "variantsweep", "errors",
+                                                        "cutoffsweep"],
                     help="c4 (default) is the benchmark line; the others print their own measurements")
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--sweep-variants", default="0,1,2", help="variantsweep: FP32C variants")
     ap.add_argument("--sweep-rows", default="0,131072,196608,262144,393216", help="variantsweep: chunk sizes")
+    ap.add_argument("--sweep-cutoffs", default="46,40,36,34,32,30",
+                    help="cutoffsweep: k of the cutoffs 2^-k * max|surplus| (46 is the default bound)")
     ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=NPTS, help="points per GPU (default: the workload's 1M)")
@@ -644,6 +674,8 @@ def main():
         run_chunksweep(args)
     elif args.workload == "variantsweep":
         run_variantsweep(args)
+    elif args.workload == "cutoffsweep":
+        run_cutoffsweep(args)
     else:
         run_gpu(args)
 

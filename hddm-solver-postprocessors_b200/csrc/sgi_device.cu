@@ -37,6 +37,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -1528,7 +1529,8 @@ struct sgi_grid
 	uint4* rec = nullptr;
 	uint2* comps = nullptr;
 	float* rowmax = nullptr;
-	float skip_below = 0.f;
+	float skip_below = 0.f;      // in use: the larger of skip_floor and the surplus cutoff
+	float skip_floor = 0.f;      // FP32C's own negligible-term bound, 2^-46 of max |surplus|
 	uint2* aux = nullptr;
 	double* s64 = nullptr;
 	float* s32 = nullptr;
@@ -1684,7 +1686,7 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 			smax = std::max(smax, m);
 		}
 		if (!rc) rc = upload((void**)&d->rowmax, rmax.data(), rmax.size() * 4);
-		d->skip_below = (float)(ldexp(smax, -46));
+		d->skip_floor = d->skip_below = (float)(ldexp(smax, -46));
 		// descent layout: groups, and per node (plus the roots' virtual
 		// parent at index nno) {first group, group count, rowmax, FP64 copy row}
 		DescentLayout D;
@@ -1733,6 +1735,20 @@ extern "C" int sgi_grid_info_get(sgi_grid_t g, sgi_grid_info* info)
 }
 
 extern "C" void sgi_grid_destroy(sgi_grid_t g) { free_grid(g); }
+
+extern "C" int sgi_grid_set_surplus_cutoff(sgi_grid_t g, double cutoff, double* effective)
+{
+	clear_error();
+	if (!g) return fail(SGI_E_INVALID, "null grid");
+	if (!g->s32) return fail(SGI_E_INVALID, "surplus cutoff: the grid has no FP32 form (build with SGI_BUILD_FP32)");
+	if (std::isnan(cutoff)) return fail(SGI_E_INVALID, "surplus cutoff is NaN");
+	// compared in FP32 with bounds computed in FP32; a cutoff above the FP32
+	// range skips every term that is not big
+	const float c = cutoff > (double)FLT_MAX ? INFINITY : (float)cutoff;
+	g->skip_below = std::max(g->skip_floor, c);
+	if (effective) *effective = g->skip_below;
+	return SGI_OK;
+}
 
 extern "C" int sgi_set_chunk_rows(int rows)
 {

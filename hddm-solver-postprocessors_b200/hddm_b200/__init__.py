@@ -69,6 +69,7 @@ def _load():
         "sgi_grid_create": (I, [P, I, U, ctypes.POINTER(P)]),
         "sgi_grid_info_get": (I, [P, ctypes.POINTER(GridInfo)]),
         "sgi_grid_destroy": (None, [P]),
+        "sgi_grid_set_surplus_cutoff": (I, [P, D, ctypes.POINTER(D)]),
         "sgi_interpolate": (I, [I, P, P, P, P, I, P]),
         "sgi_interpolate_host": (I, [I, P, P, P, P, I]),
         "sgi_backward": (I, [P, LL, P, P, P, P, P]),
@@ -254,6 +255,14 @@ class Grid:
         info = GridInfo()
         _check(lib.sgi_grid_info_get(self._h, ctypes.byref(info)))
         return info
+
+    def set_surplus_cutoff(self, cutoff):
+        """FP32C only: skip terms whose bound |w| * max|surplus row| is below
+        `cutoff` (absolute; <= 0 restores the form's own 2^-46 * max|surplus|).
+        Returns the bound in use."""
+        eff = ctypes.c_double()
+        _check(lib.sgi_grid_set_surplus_cutoff(self._h, float(cutoff), ctypes.byref(eff)))
+        return eff.value
 
     @property
     def dim(self):

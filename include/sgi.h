@@ -153,6 +153,22 @@ int sgi_grid_create(sgi_host_grid_t g, int device, unsigned flags, sgi_grid_t* o
 int sgi_grid_info_get(sgi_grid_t g, sgi_grid_info* info);
 void sgi_grid_destroy(sgi_grid_t g);
 
+/* Surplus cutoff of the FP32C form.  The reference parses a surplusCutoff
+ * parameter (LinearBasis/cpu/src/parameters.cpp:103-108,
+ * LinearBasis/cuda/src/parameters.cpp:110-127) and no kernel reads it; here
+ * it skips small terms.  The term of node n at point x is skipped, before its
+ * surplus row is read, when its bound |w_n(x)| * max_o |surplus[n][o]| (in
+ * FP32) is below `cutoff` (absolute, in surplus units), unless it is a big
+ * term (a row with an FP64 copy whose bound reaches coarse_threshold).  Each
+ * output then moves from the FP32C result by at most the sum of the bounds of
+ * the terms skipped at that point.  cutoff <= 0, the default, keeps the form's
+ * own bound of 2^-46 times the largest |surplus|, and so does any cutoff below
+ * it.  `effective` (may be NULL) receives the bound in use.  Calls and plans
+ * made afterwards use it; plans made before keep theirs.  Not to be called
+ * while another thread calls with this grid.  The FP64 form ignores it.
+ * Returns SGI_E_INVALID for a grid built without SGI_BUILD_FP32. */
+int sgi_grid_set_surplus_cutoff(sgi_grid_t g, double cutoff, double* effective);
+
 /* ---------------------------------------------------------- interpolate */
 #define SGI_FP64   0   /* plain FP64: node order and rounding of the gold kernel */
 #define SGI_FP32C  1   /* FP32 products of small terms, FP64 big terms and sums, FP64 final */

@@ -48,3 +48,11 @@ def test_library_links_no_oracle():
     assert "oracle" not in out and "libref_" not in out
     nm = subprocess.run(["nm", "-D", LIB], capture_output=True, text=True).stdout
     assert "oracle_" not in nm and "ref_interpolate" not in nm
+
+
+def test_surplus_cutoff_rejects_null_grid():
+    lib = ctypes.CDLL(LIB)
+    f = lib.sgi_grid_set_surplus_cutoff
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
+    assert f(None, 1e-3, None) == -1

@@ -381,3 +381,70 @@ def test_deep_tree_descent_and_fallback(cuda, rows):
         assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
     finally:
         H.set_chunk_rows(prev)
+
+
+def _term_bounds(index, surplus, X):
+    """|w_n(x)| * max_o |surplus[n][o]| for every point and node (FP64)."""
+    dim = index.shape[1] // 2
+    i, j = index[:, :dim].astype(np.float64), index[:, dim:].astype(np.float64)
+    rowmax = np.abs(surplus).max(axis=1)
+    out = np.zeros((len(X), len(index)))
+    for p, x in enumerate(X):
+        t = np.where(i != 0, 1.0 - np.abs(x[None, :] * i - j), 1.0)
+        out[p] = np.where((t > 0).all(axis=1), np.clip(t, 0, None).prod(axis=1), 0.0) * rowmax
+    return out
+
+
+@pytest.mark.parametrize("variant", [H.FP32C_AUTO, 4])
+def test_surplus_cutoff_error_bound(cuda, variant):
+    """A surplus cutoff moves each FP32C output from gold by at most the sum of
+    the skipped terms' bounds (plus the form's own 1e-7); cutoff <= 0 restores
+    the default bits, and a plan made before the cutoff keeps the default."""
+    import torch
+    hg = H.HostGrid.adaptive(59, 30000, 64, seed=3)
+    index, surplus = hg.arrays()
+    X = H.gen_points(59, 256, kind=2, seed=31)
+    ref = O.Gold(index, surplus).interpolate(X)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    prev = H.set_fp32c_variant(variant)
+    try:
+        x = torch.from_numpy(X).cuda()
+        base = _run(g, X, H.FP32C)
+        out_plan = torch.zeros(len(X), 64, dtype=torch.float64, device="cuda")
+        plan = H.Plan(g, x, out_plan, precision=H.FP32C)
+        plan.launch()
+        torch.cuda.synchronize()
+        plan_base = out_plan.cpu().numpy()
+        floor = g.set_surplus_cutoff(0.0)
+        assert floor == pytest.approx(np.abs(surplus).max() * 2.0 ** -46, rel=1e-6)
+        assert g.set_surplus_cutoff(floor / 4) == floor
+        smax = np.abs(surplus).max()
+        bounds = _term_bounds(index, surplus, X)
+        for k in (40, 30, 24):
+            eff = g.set_surplus_cutoff(smax * 2.0 ** -k)
+            assert eff == pytest.approx(smax * 2.0 ** -k, rel=1e-6)
+            got = _run(g, X, H.FP32C)
+            skipped = np.where(bounds < eff * (1 + 1e-5), bounds, 0.0).sum(axis=1)
+            scale = np.maximum(np.abs(ref), 1e-3 * np.abs(ref).max(axis=1, keepdims=True))
+            excess = np.abs(got - ref) - skipped[:, None] - FP32C_TOL * scale
+            assert excess.max() <= 0, (k, excess.max())
+            if k == 24:
+                assert not np.array_equal(got, base)
+        out_plan.zero_()
+        plan.launch()
+        torch.cuda.synchronize()
+        assert np.array_equal(out_plan.cpu().numpy(), plan_base)
+        assert g.set_surplus_cutoff(-1.0) == floor
+        assert np.array_equal(_run(g, X, H.FP32C), base)
+        # the FP64 form ignores it
+        g.set_surplus_cutoff(smax * 2.0 ** -10)
+        assert np.array_equal(_run(g, X), ref)
+        del plan
+    finally:
+        H.set_fp32c_variant(prev)
+
+
+def test_surplus_cutoff_needs_fp32_form(cuda):
+    g = H.Grid(H.HostGrid.regular(4, 3, 8, seed=0))
+    with pytest.raises(H.SgiError):
+        g.set_surplus_cutoff(1e-3)
