@@ -582,7 +582,7 @@ def run_multistate(args):
     dev = torch.device("cuda", 0)
     ns = 16
     hosts = [H.HostGrid.adaptive(59, 200_000, 118, seed=300 + k) for k in range(ns)]
-    grids = [H.Grid(h) for h in hosts]
+    grids = [H.Grid(h, flags=H.BUILD_FP32) for h in hosts]
     X = H.gen_points(59, ns, kind=0, seed=5)
     arr = (ctypes.c_void_p * ns)(*[g.handle.value for g in grids])
     offs = np.arange(ns + 1, dtype=np.int64)
@@ -595,6 +595,16 @@ def run_multistate(args):
     for _ in range(reps):
         rc = H.lib.sgi_interpolate_host(ns, arr, offs.ctypes.data, xh.ctypes.data, outh.ctypes.data, H.FP64)
     host_s = (time.perf_counter() - t) / reps
+    # one point on the first state, both forms
+    single = {}
+    off1 = np.array([0, 1], np.int64)
+    for name, prec in (("fp64", H.FP64), ("fp32c", H.FP32C)):
+        for _ in range(args.warmup):
+            H.lib.sgi_interpolate_host(1, arr, off1.ctypes.data, xh.ctypes.data, outh.ctypes.data, prec)
+        t = time.perf_counter()
+        for _ in range(reps):
+            H.lib.sgi_interpolate_host(1, arr, off1.ctypes.data, xh.ctypes.data, outh.ctypes.data, prec)
+        single[name] = (time.perf_counter() - t) / reps
     x = torch.from_numpy(X).to(dev)
     out = torch.empty((ns, 118), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -603,6 +613,7 @@ def run_multistate(args):
     print(json.dumps({"workload": "multistate call: 16 states x 1 point, d=59, TotalDof=118, 200k nodes per state",
                       "rc": rc, "host_call_s": host_s, "host_s_per_state": host_s / ns,
                       "graph_replay_ms": dev_ms, "graph_s_per_state": dev_ms * 1e-3 / ns,
+                      "single_point_host_call_s": single,
                       "reference_published_s_per_state": {"large, cuda (daint)": 2.754e-4,
                                                           "large, avx2 (daint)": 4.234e-3}}))
 

@@ -320,10 +320,11 @@ __device__ __forceinline__ void traverse(const GridDesc& G, const double* xs, in
 // new segment).  A chunk root's parent is one of these nodes.  Every node
 // before the end of the shallowest inactive chain node's subtree is
 // inactive, so *start moves there.
-__device__ __forceinline__ unsigned chain_state(const FwdArgs& a, int gi, const GridDesc& G, const double* xs,
-	int lane, double* wpath, int* start)
+// chain_node(d) gives the chain node at depth d + 1, d = 0..len-1.
+template <class ChainNode>
+__device__ __forceinline__ unsigned chain_state_of(ChainNode&& chain_node, int len, const GridDesc& G,
+	const double* xs, int lane, double* wpath, int* start)
 {
-	const int len = a.chain_len[gi];
 	if (len == 0) return 1u;
 	const bool mine = lane >= 1 && lane <= len;
 	bool local = true, multi = false;
@@ -331,7 +332,7 @@ __device__ __forceinline__ unsigned chain_state(const FwdArgs& a, int gi, const 
 	uint32_t skip = 0u;
 	if (mine)
 	{
-		const uint32_t node = a.chain[gi][lane - 1];
+		const uint32_t node = chain_node(lane - 1);
 		const uint4 r = __ldg(G.rec + node);
 		skip = r.x;
 		if (r.z & NODE_MULTI)
@@ -373,6 +374,13 @@ __device__ __forceinline__ unsigned chain_state(const FwdArgs& a, int gi, const 
 	const uint32_t end = __shfl_sync(FULL, skip, inactive ? __ffs(inactive) - 1 : 0);
 	if (inactive) *start = max(*start, (int)end);
 	return m;
+}
+
+// The chain of this launch's chunk start (kernel parameters) for grid gi.
+__device__ __forceinline__ unsigned chain_state(const FwdArgs& a, int gi, const GridDesc& G, const double* xs,
+	int lane, double* wpath, int* start)
+{
+	return chain_state_of([&](int d) { return a.chain[gi][d]; }, a.chain_len[gi], G, xs, lane, wpath, start);
 }
 
 // Node range of this launch for grid G.
@@ -1117,6 +1125,196 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_cols_kernel(const __grid_consta
 	}
 }
 
+// Small FP64 batches in two phases.  A point's walk takes its windows one
+// after another, and its warps then wait on their rows a few at a time; with
+// few points most of the GPU idles.  Here the walk is spread over many warps
+// and the rows are staged in bulk; the arithmetic is the gold kernel's, in
+// its order (bit-identical to fwd_f64_kernel).
+// Phase 1 (walk_chunks_kernel): one warp per (point, chunk of LCS nodes)
+// walks the chunk from its start's ancestor chain (a table built with the
+// grid), lists the chunk's hits in index order with their gold-order weights,
+// and prefetches their surplus rows into the L2.
+// Phase 2 (fwd_f64_list_kernel): one warp per (point, 32 outputs) takes the
+// point's hits chunk after chunk, copies the rows of LDEPTH hits into shared
+// memory (cp.async, one double per lane per row) and then adds them in order.
+constexpr int LCS = 2048;                  // nodes per phase-1 chunk
+constexpr int LDEPTH = 128;                // rows per phase-2 copy round
+constexpr int LBLOCK = 128;                // phase-2 threads per block
+constexpr uint32_t HIT_BAD = 0xffffffffu;  // hit count of a point with a non-finite coordinate
+
+__host__ __device__ __forceinline__ int list_stride() { return LDEPTH * 32 + LDEPTH + LDEPTH / 2; }
+
+struct ListArgs
+{
+	GridDesc g[MAXG];
+	const uint32_t* ctab[MAXG];  // per chunk k, 32 words: {chain length, chain node at depth 1..length}
+	long long ibeg[MAXG + 1];    // first (point, chunk) item of each grid; a point's items are consecutive
+	int nch[MAXG];               // chunks per grid
+	const double* x;
+	double* out;
+	uint32_t* hcnt;              // hits of item i: hcnt[i] (HIT_BAD for a non-finite point)
+	uint32_t* hnode;             //   their nodes and weights at [i * LCS, i * LCS + hcnt[i])
+	double* hw;
+	long long npts;
+	int ngrids, dim, TD;
+};
+static_assert(sizeof(ListArgs) <= 32764, "ListArgs exceeds the kernel parameter limit");
+
+__device__ __forceinline__ int list_grid(const ListArgs& a, long long p)
+{
+	int gi = 0;
+	while (gi + 1 < a.ngrids && a.g[gi + 1].pt_begin <= p) gi++;
+	return gi;
+}
+
+__global__ void __launch_bounds__(BLOCK) walk_chunks_kernel(const __grid_constant__ ListArgs a)
+{
+	extern __shared__ double smem[];
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+	double* xs = smem + warp * a.dim;
+	const long long nitems = a.ibeg[a.ngrids];
+	for (long long it = (long long)blockIdx.x * WARPS + warp; it < nitems; it += (long long)gridDim.x * WARPS)
+	{
+		int gi = 0;
+		while (gi + 1 < a.ngrids && a.ibeg[gi + 1] <= it) gi++;
+		const GridDesc& G = a.g[gi];
+		const long long loc = it - a.ibeg[gi];
+		const long long p = G.pt_begin + loc / a.nch[gi];
+		const int k = (int)(loc % a.nch[gi]);
+		bool finite = true;
+		for (int d = lane; d < a.dim; d += 32)
+		{
+			const double v = a.x[(size_t)p * a.dim + d];
+			xs[d] = v;
+			finite &= isfinite(v);
+		}
+		__syncwarp();
+		uint32_t cnt = HIT_BAD;
+		if (__all_sync(FULL, finite))
+		{
+			cnt = 0;
+			const uint32_t* ch = a.ctab[gi] + (size_t)k * 32;
+			const int len = (int)__ldg(ch);
+			int lo = k * LCS;
+			const int hi = min(G.nno, lo + LCS);
+			const unsigned pathmask = chain_state_of([&](int d) { return __ldg(ch + 1 + d); }, len, G, xs, lane,
+			                                         nullptr, &lo);
+			uint32_t* hn = a.hnode + (size_t)it * LCS;
+			double* hv = a.hw + (size_t)it * LCS;
+			const int rowb = a.TD * 8;
+			if (lo < hi)
+				traverse<false>(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&, float)
+				{
+					if ((mask >> lane) & 1u)
+					{
+						const uint32_t pos = cnt + __popc(mask & ((1u << lane) - 1u));
+						hn[pos] = (uint32_t)(n0 + lane);
+						hv[pos] = w;
+						const char* row = reinterpret_cast<const char*>(G.s64 + (size_t)(n0 + lane) * G.ld);
+						for (int b = 0; b < rowb; b += 128) asm volatile("prefetch.global.L2 [%0];" :: "l"(row + b));
+					}
+					cnt += __popc(mask);
+				}, nullptr, pathmask, len);
+		}
+		if (lane == 0) a.hcnt[it] = cnt;
+		__syncwarp();
+	}
+}
+
+__global__ void __launch_bounds__(LBLOCK) fwd_f64_list_kernel(const __grid_constant__ ListArgs a)
+{
+	extern __shared__ double smem[];
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+	double* rows = smem + (size_t)warp * list_stride();
+	double* ew = rows + LDEPTH * 32;
+	uint32_t* en = reinterpret_cast<uint32_t*>(ew + LDEPTH);
+	const uint32_t rows_s = (uint32_t)__cvta_generic_to_shared(rows) + lane * 8u;
+	const int ncb = (a.TD + 31) / 32;
+	const long long nitems = a.npts * ncb;
+	for (long long it = (long long)blockIdx.x * (LBLOCK / 32) + warp; it < nitems;
+	     it += (long long)gridDim.x * (LBLOCK / 32))
+	{
+		const long long p = it / ncb;
+		const int col = (int)(it % ncb) * 32 + lane;
+		const bool cin = col < a.TD;
+		const int gi = list_grid(a, p);
+		const GridDesc& G = a.g[gi];
+		const int nch = a.nch[gi];
+		const long long i0 = a.ibeg[gi] + (p - G.pt_begin) * nch;
+		const double* src = G.s64 + (cin ? col : 0);
+		double acc = 0.0;
+		bool ok = true;
+		// hits of chunks k0 .. k0 + 31: lane l holds chunk k0 + l's count c and
+		// the exclusive prefix excl; t of the group's T hits are taken
+		int k0 = -32;
+		uint32_t c = 0, excl = 0, T = 0, t = 0;
+		for (;;)
+		{
+			int m = 0;
+			while (m < LDEPTH)
+			{
+				if (t == T)
+				{
+					k0 += 32;
+					if (k0 >= nch) break;
+					c = k0 + lane < nch ? __ldg(a.hcnt + i0 + k0 + lane) : 0u;
+					if (__any_sync(FULL, c == HIT_BAD)) { ok = false; break; }
+					uint32_t incl = c;
+#pragma unroll
+					for (int off = 1; off < 32; off <<= 1)
+					{
+						const uint32_t v = __shfl_up_sync(FULL, incl, off);
+						if (lane >= off) incl += v;
+					}
+					T = __shfl_sync(FULL, incl, 31);
+					excl = incl - c;
+					t = 0;
+					continue;
+				}
+				const uint32_t take = min(T - t, (uint32_t)(LDEPTH - m));
+				for (uint32_t u0 = 0; u0 < take; u0 += 32)
+				{
+					const uint32_t u = u0 + lane;
+					const uint32_t h = t + u;
+					// the chunk of hit h: the last lane whose prefix is at most h
+					int sl = 0;
+#pragma unroll
+					for (int step = 16; step >= 1; step >>= 1)
+					{
+						const uint32_t v = __shfl_sync(FULL, excl, sl + step);
+						if (v <= h) sl += step;
+					}
+					const uint32_t es = __shfl_sync(FULL, excl, sl);
+					if (u < take)
+					{
+						const size_t e = (size_t)(i0 + k0 + sl) * LCS + (h - es);
+						en[m + u] = a.hnode[e];
+						ew[m + u] = a.hw[e];
+					}
+				}
+				m += (int)take;
+				t += take;
+			}
+			if (!ok || m == 0) break;
+			__syncwarp();
+			if (cin)
+			{
+				for (int q = 0; q < m; q++)
+					asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
+					             :: "r"(rows_s + (uint32_t)q * 256u), "l"(src + (size_t)en[q] * G.ld) : "memory");
+			}
+			asm volatile("cp.async.wait_all;" ::: "memory");
+			__syncwarp();
+#pragma unroll 8
+			for (int q = 0; q < m; q++) acc = __dadd_rn(acc, __dmul_rn(ew[q], rows[q * 32 + lane]));
+			__syncwarp();
+		}
+		if (cin) a.out[(size_t)p * a.TD + col] = ok ? acc : (G.nno ? __longlong_as_double(0x7ff8000000000000ll) : 0.0);
+	}
+}
+
 // Active-node count per point (single grid).
 __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ FwdArgs a, long long* counts)
 {
@@ -1378,11 +1576,13 @@ struct DeviceWork
 	cudaStream_t stream = nullptr, copy_in = nullptr, copy_out = nullptr;
 	static constexpr int NEV = 8;
 	cudaEvent_t ev_in[NEV] = {}, ev_done[NEV] = {};
-	// stream-ordered scratch of the backward pass: a private pool that keeps
-	// freed memory for the next call instead of returning it at every
-	// synchronization (as the default pool does), so repeated calls do not
-	// map their scratch again
-	cudaMemPool_t bwd_pool = nullptr;
+	// stream-ordered scratch (backward pass, small-batch hit lists): a
+	// private pool that keeps freed memory for the next call instead of
+	// returning it at every synchronization (as the default pool does), so
+	// repeated calls do not map their scratch again.  Created under its own
+	// mutex: the host-pointer entry holds mtx while it launches.
+	std::mutex pool_mtx;
+	std::atomic<cudaMemPool_t> pool{nullptr};
 };
 constexpr unsigned NCOUNTERS = 1u << 16;
 
@@ -1402,6 +1602,28 @@ int device_work(int dev, DeviceWork** out)
 		g_work[dev] = w;
 	}
 	*out = g_work[dev];
+	return SGI_OK;
+}
+
+int scratch_pool(DeviceWork* W, int dev, cudaMemPool_t* out)
+{
+	if (!W->pool.load())
+	{
+		std::lock_guard<std::mutex> lk(W->pool_mtx);
+		if (!W->pool.load())
+		{
+			cudaMemPoolProps props{};
+			props.allocType = cudaMemAllocationTypePinned;
+			props.location.type = cudaMemLocationTypeDevice;
+			props.location.id = dev;
+			cudaMemPool_t pool = nullptr;
+			CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+			uint64_t keep = UINT64_MAX;
+			CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+			W->pool.store(pool);
+		}
+	}
+	*out = W->pool.load();
 	return SGI_OK;
 }
 
@@ -1509,10 +1731,10 @@ int pick_R(int cols)
 int chunk_rows(const DeviceWork* W, const sgi_grid* g0, int precision, long long npts, int maxnno);
 
 template <class K>
-int occupancy_grid(K kernel, size_t smem, int sms, int* blocks)
+int occupancy_grid(K kernel, size_t smem, int sms, int* blocks, int block_threads = BLOCK)
 {
 	int per_sm = 0;
-	CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BLOCK, smem));
+	CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block_threads, smem));
 	if (per_sm < 1) return fail(SGI_E_CUDA, "kernel does not fit on an SM (smem %zu)", smem);
 	*blocks = per_sm * sms;
 	return SGI_OK;
@@ -1547,6 +1769,10 @@ struct sgi_grid
 	std::vector<int> parent_h;
 	std::vector<uint32_t> skip_h, depth_h;
 	std::vector<uint32_t> gfirst_h, gcount_h, gcmin_h, gpmax_h;
+	// two-phase small batches: per chunk of LCS nodes, 32 words {length of
+	// the chunk start's ancestor chain, chain node at depth 1..length}
+	uint32_t* ctab = nullptr;
+	int nlch = 0;
 	sgi_grid_info info{};
 };
 
@@ -1575,6 +1801,7 @@ void free_grid(sgi_grid* g)
 	cudaFree(g->rowmax);
 	cudaFree(g->aux);
 	cudaFree(g->grp_a); cudaFree(g->grp_b); cudaFree(g->ninfo);
+	cudaFree(g->ctab);
 	cudaSetDevice(prev);
 	delete g;
 }
@@ -1610,6 +1837,10 @@ extern "C" int sgi_device_count(void)
 	if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
 	return n;
 }
+
+namespace {
+int chain_at(const sgi_grid* g, int c0, uint32_t* out);
+} // namespace
 
 extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, sgi_grid_t* out)
 {
@@ -1653,6 +1884,13 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 	d->skip_h.resize(g.nno);
 	d->depth_h.resize(g.nno);
 	for (int n = 0; n < g.nno; n++) { d->skip_h[n] = L.rec[4 * (size_t)n]; d->depth_h[n] = L.aux[2 * (size_t)n + 1]; }
+	if (!rc && g.nno > 0)
+	{
+		d->nlch = (g.nno + LCS - 1) / LCS;
+		std::vector<uint32_t> t((size_t)d->nlch * 32, 0u);
+		for (int k = 0; k < d->nlch; k++) t[(size_t)k * 32] = (uint32_t)chain_at(d, k * LCS, &t[(size_t)k * 32 + 1]);
+		rc = upload((void**)&d->ctab, t.data(), t.size() * 4);
+	}
 	if (!rc && !(flags & SGI_BUILD_NO_FP64))
 	{
 		std::vector<double> s(nrow * d->ld, 0.0);
@@ -1867,12 +2105,96 @@ bool descent_ok(const sgi_grid_t* grids, int gb, int ng, bool chunked)
 	return true;
 }
 
+// Node-chunk size of a launch group (chunk < 0: automatic).
+int group_clen(const DeviceWork* W, const sgi_grid_t* grids, int gb, int ng, const long long* pt_offsets,
+	int precision, int chunk)
+{
+	int maxnno = 0;
+	for (int k = 0; k < ng; k++) maxnno = std::max(maxnno, grids[gb + k]->nno);
+	return chunk < 0 ? chunk_rows(W, grids[0], precision, pt_offsets[gb + ng] - pt_offsets[gb], maxnno)
+	                 : (chunk >= maxnno ? 0 : chunk);
+}
+
+// Scratch bytes of a launch group's hit lists when it runs the two-phase
+// small-batch kernels (FP64, not node-chunked, fewer points than resident
+// warps, lists within LIST_SCRATCH_MAX), else 0.
+constexpr size_t LIST_SCRATCH_MAX = 256ull << 20;
+
+size_t list_scratch(const DeviceWork* W, const sgi_grid_t* grids, int gb, int ng, const long long* pt_offsets,
+	int precision, int clen)
+{
+	const long long np = pt_offsets[gb + ng] - pt_offsets[gb];
+	if (precision != SGI_FP64 || clen || np == 0 || np >= (long long)W->sms * WARPS) return 0;
+	long long items = 0;
+	for (int k = 0; k < ng; k++) items += (pt_offsets[gb + k + 1] - pt_offsets[gb + k]) * grids[gb + k]->nlch;
+	if (items == 0) return 0;
+	const size_t bytes = (((size_t)items * 4 + 255) & ~(size_t)255) + (size_t)items * LCS * 12;
+	return bytes <= LIST_SCRATCH_MAX ? bytes : 0;
+}
+
+// The two launches of a two-phase group; buf holds list_scratch() bytes.
+int launch_lists(const DeviceWork* W, const sgi_grid_t* grids, int gb, int ng, const long long* pt_offsets,
+	const double* x, double* out, char* buf, cudaStream_t stream, int* phase2_blocks)
+{
+	const sgi_grid* g0 = grids[0];
+	const long long p0 = pt_offsets[gb];
+	ListArgs la;
+	memset(&la, 0, sizeof(la));
+	long long items = 0;
+	for (int k = 0; k < ng; k++)
+	{
+		const sgi_grid* g = grids[gb + k];
+		la.g[k] = desc_of(g, pt_offsets[gb + k] - p0, SGI_FP64);
+		la.ctab[k] = g->ctab;
+		la.nch[k] = g->nlch;
+		la.ibeg[k] = items;
+		items += (pt_offsets[gb + k + 1] - pt_offsets[gb + k]) * g->nlch;
+	}
+	la.ibeg[ng] = items;
+	la.x = x + (size_t)p0 * g0->dim;
+	la.out = out + (size_t)p0 * g0->TD;
+	la.npts = pt_offsets[gb + ng] - p0;
+	la.ngrids = ng; la.dim = g0->dim; la.TD = g0->TD;
+	la.hcnt = reinterpret_cast<uint32_t*>(buf);
+	la.hnode = reinterpret_cast<uint32_t*>(buf + (((size_t)items * 4 + 255) & ~(size_t)255));
+	la.hw = reinterpret_cast<double*>(la.hnode + (size_t)items * LCS);
+	const size_t sm1 = (size_t)WARPS * g0->dim * sizeof(double);
+	int b1 = 0;
+	int rc = occupancy_grid(walk_chunks_kernel, sm1, W->sms, &b1);
+	if (rc) return rc;
+	b1 = (int)std::min<long long>(b1, (items + WARPS - 1) / WARPS);
+	walk_chunks_kernel<<<b1, BLOCK, sm1, stream>>>(la);
+	CUDA_TRY(cudaGetLastError());
+	const size_t sm2 = (size_t)(LBLOCK / 32) * list_stride() * sizeof(double);
+	CUDA_TRY(cudaFuncSetAttribute(fwd_f64_list_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+	int b2 = 0;
+	rc = occupancy_grid(fwd_f64_list_kernel, sm2, W->sms, &b2, LBLOCK);
+	if (rc) return rc;
+	const long long items2 = la.npts * ((g0->TD + 31) / 32);
+	b2 = (int)std::min<long long>(b2, (items2 + LBLOCK / 32 - 1) / (LBLOCK / 32));
+	fwd_f64_list_kernel<<<b2, LBLOCK, sm2, stream>>>(la);
+	CUDA_TRY(cudaGetLastError());
+	*phase2_blocks = b2;
+	return SGI_OK;
+}
+
+// Pool memory handed back on the stream when the scope ends.
+struct PoolScratch
+{
+	char* p = nullptr;
+	cudaStream_t s = nullptr;
+	~PoolScratch() { if (p) cudaFreeAsync(p, s); }
+};
+
 // Launches of one forward call.  chunk < 0: the automatic chunk size; work
 // counters come from `counters` (one per launch, in order) when given, else
-// from the device workspace's ring.
+// from the device workspace's ring.  Two-phase small-batch groups take their
+// hit lists from `scratch` when given (plans), else from the device's pool;
+// while the stream is being captured without scratch they run the one-phase
+// kernels instead.
 int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets, const double* x,
 	double* out, int precision, cudaStream_t stream, int chunk = -1, unsigned long long* counters = nullptr,
-	int* nlaunch = nullptr, int variant = -1)
+	int* nlaunch = nullptr, int variant = -1, char* scratch = nullptr, size_t scratch_bytes = 0)
 {
 	if (variant < 0) variant = g_variant.load();   // may stay -1: automatic per launch group
 	const sgi_grid* g0 = grids[0];
@@ -1886,12 +2208,60 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 	// weight stack (window walk) or the group-range stack (descent)
 	if (fwd_smem(precision, g0->dim, true) > 200 * 1024) return fail(SGI_E_RANGE, "dim %d too large for shared staging", g0->dim);
 	g_stats = sgi_launch_stats{};
+	size_t lneed = 0;
+	for (int gb = 0; gb < ngrids; gb += MAXG)
+	{
+		const int ng = std::min(MAXG, ngrids - gb);
+		lneed = std::max(lneed, list_scratch(W, grids, gb, ng, pt_offsets, precision,
+		                                     group_clen(W, grids, gb, ng, pt_offsets, precision, chunk)));
+	}
+	PoolScratch pooled;
+	char* lbuf = nullptr;
+	if (lneed)
+	{
+		if (scratch) lbuf = scratch_bytes >= lneed ? scratch : nullptr;
+		else
+		{
+			cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+			CUDA_TRY(cudaStreamIsCapturing(stream, &cap));
+			if (cap == cudaStreamCaptureStatusNone)
+			{
+				cudaMemPool_t pool = nullptr;
+				rc = scratch_pool(W, g0->device, &pool);
+				if (rc) return rc;
+				void* pbuf = nullptr;
+				if (cudaMallocFromPoolAsync(&pbuf, lneed, pool, stream) == cudaSuccess)
+				{
+					lbuf = static_cast<char*>(pbuf);
+					pooled.p = lbuf;
+					pooled.s = stream;
+				}
+				else cudaGetLastError();   // no room: the one-phase kernels
+			}
+		}
+	}
 	int launches = 0;
 	for (int gb = 0; gb < ngrids; gb += MAXG)
 	{
 		const int ng = std::min(MAXG, ngrids - gb);
 		const long long p0 = pt_offsets[gb], p1 = pt_offsets[gb + ng];
 		if (p1 == p0) continue;
+		if (lbuf)
+		{
+			const int gclen = group_clen(W, grids, gb, ng, pt_offsets, precision, chunk);
+			if (list_scratch(W, grids, gb, ng, pt_offsets, precision, gclen))
+			{
+				int b2 = 0;
+				rc = launch_lists(W, grids, gb, ng, pt_offsets, x, out, lbuf, stream, &b2);
+				if (rc) return rc;
+				launches += 2;
+				g_stats.kernels += 2;
+				g_stats.grid_blocks = b2;
+				g_stats.block_threads = LBLOCK;
+				g_stats.points += p1 - p0;
+				continue;
+			}
+		}
 		FwdArgs a;
 		memset(&a, 0, sizeof(a));
 		for (int k = 0; k < ng; k++) a.g[k] = desc_of(grids[gb + k], pt_offsets[gb + k] - p0, precision);
@@ -1901,7 +2271,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 		a.ngrids = ng; a.dim = g0->dim; a.TD = g0->TD;
 		int maxnno = 0;
 		for (int k = 0; k < ng; k++) maxnno = std::max(maxnno, grids[gb + k]->nno);
-		const int clen = chunk < 0 ? chunk_rows(W, g0, precision, a.npts, maxnno) : (chunk >= maxnno ? 0 : chunk);
+		const int clen = group_clen(W, grids, gb, ng, pt_offsets, precision, chunk);
 		const int nchunks = clen ? (maxnno + clen - 1) / clen : 1;
 		const bool descent = precision == SGI_FP32C && descent_ok(grids, gb, ng, clen > 0);
 		const bool small = a.npts < (long long)W->sms * WARPS;
@@ -1941,11 +2311,15 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 	return SGI_OK;
 }
 
-// Launch count of a forward call with chunk size `chunk` (as launch_forward).
-int count_launches(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets, int chunk)
+// Launch count of a forward call with chunk size `chunk` >= 0 (as
+// launch_forward given the scratch its two-phase groups need), and that
+// scratch in *list_bytes.
+int count_launches(const DeviceWork* W, int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	int precision, int chunk, size_t* list_bytes)
 {
 	int n = 0;
 	const int passes = (grids[0]->TD + PASS - 1) / PASS;
+	*list_bytes = 0;
 	for (int gb = 0; gb < ngrids; gb += MAXG)
 	{
 		const int ng = std::min(MAXG, ngrids - gb);
@@ -1953,7 +2327,9 @@ int count_launches(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 		int maxnno = 0;
 		for (int k = 0; k < ng; k++) maxnno = std::max(maxnno, grids[gb + k]->nno);
 		const int clen = chunk >= maxnno ? 0 : chunk;
-		n += passes * (clen ? (maxnno + clen - 1) / clen : 1);
+		const size_t lb = list_scratch(W, grids, gb, ng, pt_offsets, precision, clen);
+		*list_bytes = std::max(*list_bytes, lb);
+		n += lb ? 2 : passes * (clen ? (maxnno + clen - 1) / clen : 1);
 	}
 	return n;
 }
@@ -2122,24 +2498,10 @@ extern "C" int sgi_backward(sgi_grid_t g, long long npts, const double* x, const
 	a.G = desc_of(g, 0);
 	a.x = x; a.gout = gout; a.gx = gx; a.npts = npts; a.dim = g->dim; a.TD = g->TD;
 
-	// scratch (stream-ordered allocations from the device's backward pool)
-	if (!W->bwd_pool)
-	{
-		std::lock_guard<std::mutex> lk(W->mtx);
-		if (!W->bwd_pool)
-		{
-			cudaMemPoolProps props{};
-			props.allocType = cudaMemAllocationTypePinned;
-			props.location.type = cudaMemLocationTypeDevice;
-			props.location.id = g->device;
-			cudaMemPool_t pool = nullptr;
-			CUDA_TRY(cudaMemPoolCreate(&pool, &props));
-			uint64_t keep = UINT64_MAX;
-			CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-			W->bwd_pool = pool;
-		}
-	}
-	cudaMemPool_t pool = W->bwd_pool;
+	// scratch (stream-ordered allocations from the device's pool)
+	cudaMemPool_t pool = nullptr;
+	rc = scratch_pool(W, g->device, &pool);
+	if (rc) return rc;
 	long long* counts = nullptr;
 	long long* offs = nullptr;
 	uint32_t *pn = nullptr, *node_sorted = nullptr;
@@ -2335,6 +2697,8 @@ struct sgi_plan
 	int variant = 0;
 	int launches = 0;
 	unsigned long long* counters = nullptr;
+	char* scratch = nullptr;          // hit lists of two-phase small-batch groups
+	size_t scratch_bytes = 0;
 	cudaGraph_t graph = nullptr;
 	cudaGraphExec_t exec = nullptr;
 	float tuned_ms = 0.f;
@@ -2386,6 +2750,7 @@ void free_plan(sgi_plan* p)
 	if (p->exec) cudaGraphExecDestroy(p->exec);
 	if (p->graph) cudaGraphDestroy(p->graph);
 	if (p->counters) cudaFree(p->counters);
+	if (p->scratch) cudaFree(p->scratch);
 	delete p;
 }
 
@@ -2465,9 +2830,16 @@ extern "C" int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long l
 	p->variant = variant;
 	p->chunk = chunk;
 	p->tuned_ms = tuned;
-	p->launches = count_launches(ngrids, grids, pt_offsets, chunk);
+	size_t list_bytes = 0;
+	p->launches = count_launches(W, ngrids, grids, pt_offsets, precision, chunk, &list_bytes);
 	cudaError_t e = cudaMalloc(&p->counters, sizeof(unsigned long long) * std::max(p->launches, 1));
 	if (e != cudaSuccess) { free_plan(p); return fail(SGI_E_NOMEM, "cudaMalloc failed: %s", cudaGetErrorString(e)); }
+	if (list_bytes)
+	{
+		e = cudaMalloc(&p->scratch, list_bytes);
+		if (e != cudaSuccess) { free_plan(p); return fail(SGI_E_NOMEM, "cudaMalloc failed: %s", cudaGetErrorString(e)); }
+		p->scratch_bytes = list_bytes;
+	}
 	cudaStream_t cs = nullptr;
 	e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
 	if (e != cudaSuccess) { free_plan(p); return fail(SGI_E_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e)); }
@@ -2475,7 +2847,8 @@ extern "C" int sgi_plan_create(int ngrids, const sgi_grid_t* grids, const long l
 	if (e == cudaSuccess)
 	{
 		int n = 0;
-		rc = launch_forward(ngrids, grids, pt_offsets, x, out, precision, cs, chunk, p->counters, &n, variant);
+		rc = launch_forward(ngrids, grids, pt_offsets, x, out, precision, cs, chunk, p->counters, &n, variant,
+		                    p->scratch, p->scratch_bytes);
 		cudaGraph_t g = nullptr;
 		e = cudaStreamEndCapture(cs, &g);
 		p->graph = g;

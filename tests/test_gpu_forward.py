@@ -448,3 +448,67 @@ def test_surplus_cutoff_needs_fp32_form(cuda):
     g = H.Grid(H.HostGrid.regular(4, 3, 8, seed=0))
     with pytest.raises(H.SgiError):
         g.set_surplus_cutoff(1e-3)
+
+
+def _deep_subtree_grid(td, seed):
+    """A containment chain of depth 46 (_deep_chain_grid over 52 dimensions)
+    whose deepest node holds a regular level-5 grid over dimensions 45-51
+    (2,464 nodes at depths 47 to 51), placed right after it: the node chunk
+    starting at 2,048 then lies below the 31 stored chain levels."""
+    dim = 52
+    idx, _ = _deep_chain_grid(dim, 46, td, seed)
+    sub, _ = H.HostGrid.regular(7, 5, 1, seed=0).arrays()
+    sub = sub[(sub[:, :7] != 0).any(axis=1)]          # the subtree root is the chain's last node
+    rows = np.zeros((len(sub), 2 * dim), np.int32)
+    rows[:, :45] = 2                                   # inside the last chain node (i = 2, j = 0, dims 0-44)
+    rows[:, 45:52] = sub[:, :7]
+    rows[:, dim + 45:dim + 52] = sub[:, 7:]
+    idx = np.concatenate([idx[:46], rows, idx[46:]])
+    lev = np.where(idx[:, :dim] > 0, 1, 0).sum(axis=1)
+    sur = np.random.default_rng(seed).uniform(-1, 1, (len(idx), td)) * 2.0 ** (-lev[:, None])
+    return idx, sur
+
+
+@pytest.mark.parametrize("case", ["adaptive", "permuted", "dead", "deep"])
+def test_small_batch_two_phase_exact(cuda, case):
+    """Small FP64 batches walk node chunks of 2,048 in parallel and then add
+    the listed hits in order: bit-identical to gold across chunk boundaries
+    (grids in random order with many tree roots, never-active nodes between
+    live ones, chunk starts deeper than the stored ancestor chains), through
+    direct calls, a graph plan and the host-pointer entry, for one point and
+    for a few hundred."""
+    import torch
+    if case == "deep":
+        idx, sur = _deep_subtree_grid(40, seed=5)
+        rng = np.random.default_rng(6)
+        X = rng.uniform(0.0, 1.0, (300, 52))
+        X[:, :45] *= 0.5                                # inside the chain ...
+        X[::4, rng.integers(0, 45, 75)] = 0.8           # ... or leaving it
+    else:
+        idx, sur = H.HostGrid.adaptive(8, 9000, 40, seed=7).arrays()
+        if case == "permuted":
+            perm = np.random.default_rng(1).permutation(len(idx))
+            idx, sur = idx[perm], sur[perm]
+        elif case == "dead":
+            dead = np.zeros((5, idx.shape[1]), np.int32)
+            dead[:, 8:] = 3                             # i = 0, j = 3: never active
+            at = [0, 2047, 2048, 4000, 8999]
+            idx = np.insert(idx, at, dead, axis=0)
+            sur = np.insert(sur, at, np.ones((5, sur.shape[1])), axis=0)
+        X = H.gen_points(8, 300, kind=2, seed=9)
+    hg = H.HostGrid.from_dense(idx, sur)
+    g = H.Grid(hg)
+    assert g.nno > 2048
+    if case == "deep":
+        assert g.info.tree_depth > 32
+    ref = O.Gold(idx, sur).interpolate(X)
+    assert np.array_equal(_run(g, X), ref)
+    assert np.array_equal(_run(g, X[:1]), ref[:1])
+    assert np.array_equal(H.interpolate_host(g, X), ref)
+    x = torch.from_numpy(X).cuda()
+    out = torch.zeros(len(X), sur.shape[1], dtype=torch.float64, device="cuda")
+    plan = H.Plan(g, x, out, precision=H.FP64)
+    plan.launch()
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), ref)
+    del plan
