@@ -1137,9 +1137,9 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_cols_kernel(const __grid_consta
 // Phase 2 (fwd_f64_list_kernel): one warp per (point, 32 outputs) takes the
 // point's hits chunk after chunk, copies the rows of LDEPTH hits into shared
 // memory (cp.async, one double per lane per row) and then adds them in order.
-constexpr int LCS = 2048;                  // nodes per phase-1 chunk
-constexpr int LDEPTH = 128;                // rows per phase-2 copy round
-constexpr int LBLOCK = 128;                // phase-2 threads per block
+constexpr int LCS = 512;                   // nodes per phase-1 chunk
+constexpr int LDEPTH = 256;                // rows per phase-2 copy round
+constexpr int LBLOCK = 64;                 // phase-2 threads per block
 constexpr uint32_t HIT_BAD = 0xffffffffu;  // hit count of a point with a non-finite coordinate
 
 __host__ __device__ __forceinline__ int list_stride() { return LDEPTH * 32 + LDEPTH + LDEPTH / 2; }
@@ -1274,10 +1274,13 @@ __global__ void __launch_bounds__(LBLOCK) fwd_f64_list_kernel(const __grid_const
 					continue;
 				}
 				const uint32_t take = min(T - t, (uint32_t)(LDEPTH - m));
-				for (uint32_t u0 = 0; u0 < take; u0 += 32)
+				// list positions of hits t .. t + take - 1 first, then all their
+				// loads, then the stores: one round trip for the whole take
+				size_t e[LDEPTH / 32];
+#pragma unroll
+				for (int j = 0; j < LDEPTH / 32; j++)
 				{
-					const uint32_t u = u0 + lane;
-					const uint32_t h = t + u;
+					const uint32_t h = t + (uint32_t)(j * 32 + lane);
 					// the chunk of hit h: the last lane whose prefix is at most h
 					int sl = 0;
 #pragma unroll
@@ -1287,13 +1290,24 @@ __global__ void __launch_bounds__(LBLOCK) fwd_f64_list_kernel(const __grid_const
 						if (v <= h) sl += step;
 					}
 					const uint32_t es = __shfl_sync(FULL, excl, sl);
-					if (u < take)
-					{
-						const size_t e = (size_t)(i0 + k0 + sl) * LCS + (h - es);
-						en[m + u] = a.hnode[e];
-						ew[m + u] = a.hw[e];
-					}
+					e[j] = (size_t)(i0 + k0 + sl) * LCS + (h - es);
 				}
+				uint32_t nd[LDEPTH / 32];
+				double wv[LDEPTH / 32];
+#pragma unroll
+				for (int j = 0; j < LDEPTH / 32; j++)
+				{
+					const bool in = (uint32_t)(j * 32 + lane) < take;
+					nd[j] = in ? a.hnode[e[j]] : 0u;
+					wv[j] = in ? a.hw[e[j]] : 0.0;
+				}
+#pragma unroll
+				for (int j = 0; j < LDEPTH / 32; j++)
+					if ((uint32_t)(j * 32 + lane) < take)
+					{
+						en[m + j * 32 + lane] = nd[j];
+						ew[m + j * 32 + lane] = wv[j];
+					}
 				m += (int)take;
 				t += take;
 			}
