@@ -1133,7 +1133,10 @@ __global__ void __launch_bounds__(BLOCK) fwd_f64_cols_kernel(const __grid_consta
 // Phase 1 (walk_chunks_kernel): one warp per (point, chunk of LCS nodes)
 // walks the chunk from its start's ancestor chain (a table built with the
 // grid), lists the chunk's hits in index order with their gold-order weights,
-// and prefetches their surplus rows into the L2.
+// and prefetches their surplus rows into the L2.  For the FP32C form (grid
+// descriptors with row maxima) it lists only the terms the FP32C kernels keep
+// (big terms, and others whose bound reaches the dropped-term bound); their
+// FP64 rows are then added exactly.
 // Phase 2 (fwd_f64_list_kernel): one warp per (point, 32 outputs) takes the
 // point's hits chunk after chunk, copies the rows of LDEPTH hits into shared
 // memory (cp.async, one double per lane per row) and then adds them in order.
@@ -1204,17 +1207,24 @@ __global__ void __launch_bounds__(BLOCK) walk_chunks_kernel(const __grid_constan
 			double* hv = a.hw + (size_t)it * LCS;
 			const int rowb = a.TD * 8;
 			if (lo < hi)
-				traverse<false>(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4&, float)
+				traverse<false>(G, xs, lane, lo, hi, [&](unsigned mask, int n0, double w, const uint4& r, float rm)
 				{
-					if ((mask >> lane) & 1u)
+					bool keep = (mask >> lane) & 1u;
+					if (keep && G.rowmax)
 					{
-						const uint32_t pos = cnt + __popc(mask & ((1u << lane) - 1u));
+						const float bound = fabsf(__double2float_rn(w)) * rm;
+						keep = ((r.z & NODE_COARSE) && bound >= G.big_below) || bound >= G.skip_below;
+					}
+					const unsigned km = __ballot_sync(FULL, keep);
+					if (keep)
+					{
+						const uint32_t pos = cnt + __popc(km & ((1u << lane) - 1u));
 						hn[pos] = (uint32_t)(n0 + lane);
 						hv[pos] = w;
 						const char* row = reinterpret_cast<const char*>(G.s64 + (size_t)(n0 + lane) * G.ld);
 						for (int b = 0; b < rowb; b += 128) asm volatile("prefetch.global.L2 [%0];" :: "l"(row + b));
 					}
-					cnt += __popc(mask);
+					cnt += __popc(km);
 				}, nullptr, pathmask, len);
 		}
 		if (lane == 0) a.hcnt[it] = cnt;
@@ -2130,17 +2140,23 @@ int group_clen(const DeviceWork* W, const sgi_grid_t* grids, int gb, int ng, con
 }
 
 // Scratch bytes of a launch group's hit lists when it runs the two-phase
-// small-batch kernels (FP64, not node-chunked, fewer points than resident
-// warps, lists within LIST_SCRATCH_MAX), else 0.
+// small-batch kernels (FP64, or FP32C on grids that keep their FP64 rows; not
+// node-chunked; fewer points than resident warps; lists within
+// LIST_SCRATCH_MAX), else 0.
 constexpr size_t LIST_SCRATCH_MAX = 256ull << 20;
 
 size_t list_scratch(const DeviceWork* W, const sgi_grid_t* grids, int gb, int ng, const long long* pt_offsets,
 	int precision, int clen)
 {
 	const long long np = pt_offsets[gb + ng] - pt_offsets[gb];
-	if (precision != SGI_FP64 || clen || np == 0 || np >= (long long)W->sms * WARPS) return 0;
+	if ((precision != SGI_FP64 && precision != SGI_FP32C) || clen || np == 0 || np >= (long long)W->sms * WARPS)
+		return 0;
 	long long items = 0;
-	for (int k = 0; k < ng; k++) items += (pt_offsets[gb + k + 1] - pt_offsets[gb + k]) * grids[gb + k]->nlch;
+	for (int k = 0; k < ng; k++)
+	{
+		if (!grids[gb + k]->s64) return 0;
+		items += (pt_offsets[gb + k + 1] - pt_offsets[gb + k]) * grids[gb + k]->nlch;
+	}
 	if (items == 0) return 0;
 	const size_t bytes = (((size_t)items * 4 + 255) & ~(size_t)255) + (size_t)items * LCS * 12;
 	return bytes <= LIST_SCRATCH_MAX ? bytes : 0;
@@ -2148,7 +2164,7 @@ size_t list_scratch(const DeviceWork* W, const sgi_grid_t* grids, int gb, int ng
 
 // The two launches of a two-phase group; buf holds list_scratch() bytes.
 int launch_lists(const DeviceWork* W, const sgi_grid_t* grids, int gb, int ng, const long long* pt_offsets,
-	const double* x, double* out, char* buf, cudaStream_t stream, int* phase2_blocks)
+	const double* x, double* out, int precision, char* buf, cudaStream_t stream, int* phase2_blocks)
 {
 	const sgi_grid* g0 = grids[0];
 	const long long p0 = pt_offsets[gb];
@@ -2158,7 +2174,7 @@ int launch_lists(const DeviceWork* W, const sgi_grid_t* grids, int gb, int ng, c
 	for (int k = 0; k < ng; k++)
 	{
 		const sgi_grid* g = grids[gb + k];
-		la.g[k] = desc_of(g, pt_offsets[gb + k] - p0, SGI_FP64);
+		la.g[k] = desc_of(g, pt_offsets[gb + k] - p0, precision);
 		la.ctab[k] = g->ctab;
 		la.nch[k] = g->nlch;
 		la.ibeg[k] = items;
@@ -2266,7 +2282,7 @@ int launch_forward(int ngrids, const sgi_grid_t* grids, const long long* pt_offs
 			if (list_scratch(W, grids, gb, ng, pt_offsets, precision, gclen))
 			{
 				int b2 = 0;
-				rc = launch_lists(W, grids, gb, ng, pt_offsets, x, out, lbuf, stream, &b2);
+				rc = launch_lists(W, grids, gb, ng, pt_offsets, x, out, precision, lbuf, stream, &b2);
 				if (rc) return rc;
 				launches += 2;
 				g_stats.kernels += 2;

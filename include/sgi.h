@@ -181,12 +181,13 @@ int sgi_grid_set_surplus_cutoff(sgi_grid_t g, double cutoff, double* effective);
  * (LinearBasis/cuda/src/InterpolateArray.cu:239-267, one point per call) and
  * ..._InterpolateArrayManyMultistate (InterpolateArrayManyMultistate.cu:346-395,
  * one point per state per call).
- * Small FP64 batches (fewer points than the GPU holds warps) walk node chunks
- * in parallel into hit lists, 12 bytes per (point, node), at most 256 MB per
- * call, taken from a per-device stream-ordered pool that keeps freed memory
- * for later calls (plans own theirs).  While `stream` is being captured
- * outside a plan, or when the lists would not fit, they run the one-phase
- * kernels instead (same bits). */
+ * Small batches (fewer points than the GPU holds warps; FP32C only on grids
+ * that keep their FP64 rows) walk node chunks in parallel into hit lists,
+ * 12 bytes per (point, node), at most 256 MB per call, taken from a
+ * per-device stream-ordered pool that keeps freed memory for later calls
+ * (plans own theirs); FP32C then adds the FP64 rows of the terms it keeps.
+ * While `stream` is being captured outside a plan, or when the lists would
+ * not fit, they run the one-phase kernels instead (FP64: same bits). */
 int sgi_interpolate(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
 	const double* x, double* out, int precision, void* stream);
 

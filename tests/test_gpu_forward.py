@@ -276,13 +276,16 @@ def test_fp32c_variants_within_tolerance(cuda, variant, td, rows):
     """Every FP32C kernel variant (E = 1, 2 and 4 output layouts, one and two
     output passes, chunked or not; 0-2 walk by descent, 4 forces the window
     walk) stays within the FP32C tolerance of gold, and the FP64 form stays
-    bit-exact under the same settings."""
+    bit-exact under the same settings.  The FP32C grid keeps no FP64 rows, so
+    that this small batch runs the FP32C kernels (with FP64 rows it would run
+    the two-phase small-batch kernels)."""
     h = H.HostGrid.adaptive(59, 6000, td, seed=60 + td)
     g = H.Grid(h, flags=H.BUILD_FP32)
+    g32 = H.Grid(h, flags=H.BUILD_FP32 | H.BUILD_NO_FP64)
     X = H.gen_points(59, 700, kind=2, seed=61)
     prev, prev_v = H.set_chunk_rows(rows), H.set_fp32c_variant(variant)
     try:
-        out32 = _run(g, X, H.FP32C)
+        out32 = _run(g32, X, H.FP32C)
         out64 = _run(g, X, H.FP64)
     finally:
         H.set_chunk_rows(prev)
@@ -365,11 +368,13 @@ def _deep_chain_grid(dim, depth, td, seed):
 def test_deep_tree_descent_and_fallback(cuda, rows):
     """A containment tree of depth 46: the FP32C descent handles it whole
     (depth <= 64); in node chunks (chains must be complete, depth <= 32) the
-    window walk takes over.  FP64 bit-exact, FP32C within tolerance."""
+    window walk takes over.  FP64 bit-exact, FP32C within tolerance (on a
+    grid without FP64 rows, so that this small batch runs the FP32C kernels)."""
     dim, depth = 48, 46
     idx, sur = _deep_chain_grid(dim, depth, 64, seed=3)
     hg = H.HostGrid.from_dense(idx, sur)
-    g = H.Grid(hg, flags=H.BUILD_FP32)
+    g = H.Grid(hg)
+    g32 = H.Grid(hg, flags=H.BUILD_FP32 | H.BUILD_NO_FP64)
     assert g.info.tree_depth == depth
     rng = np.random.default_rng(4)
     X = rng.uniform(0.0, 0.5, (400, dim))          # deep in the chain ...
@@ -378,7 +383,7 @@ def test_deep_tree_descent_and_fallback(cuda, rows):
     prev = H.set_chunk_rows(rows)
     try:
         assert np.array_equal(_run(g, X), ref)
-        assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
+        assert O.rel_error(_run(g32, X, H.FP32C), ref)[0] <= FP32C_TOL
     finally:
         H.set_chunk_rows(prev)
 
@@ -395,17 +400,21 @@ def _term_bounds(index, surplus, X):
     return out
 
 
-@pytest.mark.parametrize("variant", [H.FP32C_AUTO, 4])
-def test_surplus_cutoff_error_bound(cuda, variant):
+@pytest.mark.parametrize("variant,flags", [(H.FP32C_AUTO, H.BUILD_FP32),
+                                           (H.FP32C_AUTO, H.BUILD_FP32 | H.BUILD_NO_FP64),
+                                           (4, H.BUILD_FP32 | H.BUILD_NO_FP64)])
+def test_surplus_cutoff_error_bound(cuda, variant, flags):
     """A surplus cutoff moves each FP32C output from gold by at most the sum of
     the skipped terms' bounds (plus the form's own 1e-7); cutoff <= 0 restores
-    the default bits, and a plan made before the cutoff keeps the default."""
+    the default bits, and a plan made before the cutoff keeps the default.
+    With FP64 rows kept, this small batch runs the two-phase kernels; without
+    them the descent (automatic variant) or the window walk (variant 4)."""
     import torch
     hg = H.HostGrid.adaptive(59, 30000, 64, seed=3)
     index, surplus = hg.arrays()
     X = H.gen_points(59, 256, kind=2, seed=31)
     ref = O.Gold(index, surplus).interpolate(X)
-    g = H.Grid(hg, flags=H.BUILD_FP32)
+    g = H.Grid(hg, flags=flags)
     prev = H.set_fp32c_variant(variant)
     try:
         x = torch.from_numpy(X).cuda()
@@ -436,9 +445,10 @@ def test_surplus_cutoff_error_bound(cuda, variant):
         assert np.array_equal(out_plan.cpu().numpy(), plan_base)
         assert g.set_surplus_cutoff(-1.0) == floor
         assert np.array_equal(_run(g, X, H.FP32C), base)
-        # the FP64 form ignores it
-        g.set_surplus_cutoff(smax * 2.0 ** -10)
-        assert np.array_equal(_run(g, X), ref)
+        if not flags & H.BUILD_NO_FP64:
+            # the FP64 form ignores it
+            g.set_surplus_cutoff(smax * 2.0 ** -10)
+            assert np.array_equal(_run(g, X), ref)
         del plan
     finally:
         H.set_fp32c_variant(prev)
@@ -497,13 +507,16 @@ def test_small_batch_two_phase_exact(cuda, case):
             sur = np.insert(sur, at, np.ones((5, sur.shape[1])), axis=0)
         X = H.gen_points(8, 300, kind=2, seed=9)
     hg = H.HostGrid.from_dense(idx, sur)
-    g = H.Grid(hg)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
     assert g.nno > 2048
     if case == "deep":
         assert g.info.tree_depth > 32
     ref = O.Gold(idx, sur).interpolate(X)
     assert np.array_equal(_run(g, X), ref)
     assert np.array_equal(_run(g, X[:1]), ref[:1])
+    # FP32C: the same kernels add the FP64 rows of the terms FP32C keeps
+    # (dropped: bound below 2^-46 of the largest surplus)
+    assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
     assert np.array_equal(H.interpolate_host(g, X), ref)
     x = torch.from_numpy(X).cuda()
     out = torch.zeros(len(X), sur.shape[1], dtype=torch.float64, device="cuda")
