@@ -125,3 +125,74 @@ def test_two_rank_gloo_sharded_backward():
     gx_equal, gs_rel = ret.get(timeout=10)
     assert gx_equal
     assert gs_rel <= 1e-13
+
+
+def test_shard_states_assigns_every_state_once():
+    from hddm_b200.shard import shard_states, state_rows
+    costs = [50, 0, 70, 10, 40, 40, 5]
+    for world in (1, 2, 3, 8):
+        owned = shard_states(costs, world)
+        assert len(owned) == world
+        flat = sorted(s for o in owned for s in o)
+        assert flat == list(range(len(costs)))
+        assert all(o == sorted(o) for o in owned)
+        assert owned == shard_states(costs, world)               # deterministic
+    # largest first to the least loaded rank: 70 | 50 | 40+40 ... for 3 ranks
+    loads = [sum(costs[s] for s in o) for o in shard_states(costs, 3)]
+    assert max(loads) - min(loads) <= max(costs)
+    assert shard_states([], 2) == [[], []]
+    with pytest.raises(ValueError):
+        shard_states(costs, 0)
+    counts = [3, 0, 2, 4]
+    assert state_rows([2, 0], counts).tolist() == [3, 4, 0, 1, 2]
+    assert state_rows([1], counts).tolist() == []
+
+
+def _state_worker(rank, world, port, ret):
+    import sys
+    import torch
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in (root, os.path.join(root, "hddm-solver-postprocessors_b200")):
+        sys.path.insert(0, p)
+    import hddm_b200 as H
+    import oracle as O
+    from hddm_b200.shard import gather_state_outputs, shard_states, state_rows
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    nnos = [900, 3000, 400, 1500, 2200]
+    counts = [3, 0, 7, 1, 4]
+    X = H.gen_points(10, sum(counts), kind=2, seed=8)
+    owned = shard_states([c * n for c, n in zip(counts, nnos)], world)
+    # a rank builds only the grids of its own states
+    parts = []
+    for s in owned[rank]:
+        hg = H.HostGrid.adaptive(10, nnos[s], 12, seed=30 + s)
+        parts.append(O.Gold(*hg.arrays()).interpolate(X[state_rows([s], counts)]))
+    local = torch.from_numpy(np.concatenate(parts) if parts else np.zeros((0, 12)))
+    full = gather_state_outputs(local, owned, counts)
+    if rank == 0:
+        ref = np.concatenate([O.Gold(*H.HostGrid.adaptive(10, nnos[s], 12, seed=30 + s).arrays())
+                              .interpolate(X[state_rows([s], counts)]) for s in range(len(nnos))])
+        ret.put((bool(np.array_equal(full.numpy(), ref)), [len(o) for o in owned]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_gloo_whole_state_sharding():
+    """A multistate set split by whole states: each rank holds only its own
+    states' grids, evaluates all their points, and the gathered outputs equal
+    the whole batch in its own row order."""
+    ctx = mp.get_context("spawn")
+    ret = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_state_worker, args=(r, 2, port, ret)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    equal, per_rank = ret.get(timeout=10)
+    assert equal
+    assert sum(per_rank) == 5 and min(per_rank) >= 1
