@@ -268,7 +268,8 @@ int sgi_set_fp32c_variant(int variant);
 /* Plans: one forward call recorded into a CUDA graph and replayed.
  * sgi_plan_create records every launch of sgi_interpolate(ngrids, grids,
  * pt_offsets, x, out, precision) (work-counter clears and node-chunk launches,
- * with work counters owned by the plan) into a graph; sgi_plan_launch replays
+ * with work counters, and the hit lists of small batches, owned by the plan)
+ * into a graph; sgi_plan_launch replays
  * it on `stream` with one cudaGraphLaunch.  x and out are baked into the
  * graph: later replays read the same x buffer and write the same out buffer.
  * chunk_rows >= 0 fixes the node-chunk size (0 = none); chunk_rows < 0 lets the
