@@ -222,7 +222,10 @@ int sgi_backward(sgi_grid_t g, long long npts, const double* x, const double* go
  * until the process exits.
  *
  * Arguments and results are those of sgi_interpolate (device x and out, host
- * pt_offsets).  A call makes ceil(ngrids / 48) * ceil(TotalDof / 256) kernel
+ * pt_offsets); FP64 results are bit-identical to it.  Small batches run the
+ * one-phase kernels here (sgi_interpolate's two-phase ones need scratch), so
+ * small FP32C batches may differ from sgi_interpolate's in the last bits
+ * (both within the FP32C tolerance).  A call makes ceil(ngrids / 48) * ceil(TotalDof / 256) kernel
  * launches (groups of grids with no points are skipped); a call that would need
  * more than SGI_NOALLOC_MAX_LAUNCHES launches is rejected with SGI_E_RANGE
  * before anything is launched.  The first call on each device looks up the
