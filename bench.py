@@ -1,6 +1,6 @@
 """Benchmark of the sparse-grid interpolation hot path on B200.
 
-Workload (one GPU): one adaptive d=59 grid of 1,000,000 nodes grown by seeded
+Workload (per GPU): one adaptive d=59 grid of 1,000,000 nodes grown by seeded
 random refinement (levels <= 7), TotalDof = 256, and 1,000,000 query points
 (first half uniform in [0,1]^59, second half N(0.5, 0.05^2) clipped to [0,1]).
 A step is one forward pass over all points.  The headline form is the batched
@@ -9,18 +9,22 @@ the reference's gold path) is timed beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-With N > 1 (one process per GPU under torchrun) every rank replicates the grid
-and evaluates its own 1M points (weak scaling, no collective on the data path).
-`--impl reference` times the reference's own CPU code (oracle/_ref, compiled
-from the reference sources) on the host cores over a bounded sample of points.
+With N > 1 the benchmark runs one process per GPU: under torchrun (RANK /
+WORLD_SIZE set) it is one of them; started directly it launches torchrun
+itself.  Every rank replicates the grid and evaluates its own 1M points (weak
+scaling, no collective on the data path; NCCL carries only the barrier and the
+max-over-ranks timing).  `--impl reference` times the reference's own CPU code
+(oracle/_ref, compiled from the reference sources) on the host cores over a
+bounded sample of points per step, building its grid file and points with the
+oracle's generator so that the product library is never loaded.
 """
 import argparse
 import json
 import os
+import socket
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -33,8 +37,25 @@ for _p in (ROOT, PKG):
 
 DIM, NNO, TD, NPTS = 59, 1_000_000, 256, 1_000_000
 GRID_SEED, POINT_SEED = 4, 40
+CHECK_POINTS, CHECK_SEED = 4096, 40
 METRIC = "d=59 points/s: batched FP32+comp vs plain FP64 GPU @<=1e-7 rel err; %HBM peak"
 WORKLOAD = "C4: d=59 adaptive grid, 1M nodes (levels<=7), TotalDof=256, 1M points (half U[0,1], half N(0.5,0.05^2))"
+
+# Random 1 KB surplus-row gathers from an L2-resident region with 16-byte
+# loads, measured on this pool's B200s by a standalone probe: 20.1 TB/s with 64
+# warps per SM, 14.6 TB/s with 32 (four blocks of eight warps, the occupancy
+# of the forward kernels' default variant).
+GATHER_PEAK_TBS = {64: 20.1, 32: 14.6}
+# Warps per SM of the FP32C kernel variants (blocks per SM x 8 warps).
+VARIANT_WARPS = {0: 24, 1: 32, 2: 16}
+
+# DRAM bytes (read + write) of one FP32C forward call of the default workload,
+# keyed by (node-chunk rows, kernel variant): the sum over the call's
+# fwd_f32d_kernel launches from ncu captures of the same chunking on 65,536
+# and 131,072 points, fitted as a + b * points and taken at 1M points (the
+# per-chunk row reads do not grow with the points; outputs, coordinates and
+# L2 misses do).
+FP32C_CALL_DRAM_BYTES = {}
 
 
 def env_rank():
@@ -49,6 +70,11 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def check_subsample():
+    """The fixed 4,096-point subsample (seed 40) the oracle checks."""
+    return np.sort(np.random.Generator(np.random.PCG64(CHECK_SEED)).choice(NPTS, CHECK_POINTS, replace=False))
+
+
 def make_workload(npts=NPTS, seed_offset=0):
     import hddm_b200 as H
     t = time.time()
@@ -57,8 +83,11 @@ def make_workload(npts=NPTS, seed_offset=0):
     return hg, X, time.time() - t
 
 
-def alg_bytes(hg, info, npts, s_b):
-    """SURVEY 8(d) algorithmic bytes of one launch (each grid counted once)."""
+def alg_bytes(hg, info, npts, fp32c):
+    """Algorithmic bytes of one forward call, each grid array counted once:
+    coordinates and outputs (FP64) per point, the surplus rows (FP32 for FP32C,
+    FP64 for the FP64 form), for FP32C the FP64 copies of the coarse rows,
+    chains (2 B per node per non-constant dimension) and unique xps (4 B)."""
     idx, _ = hg.arrays()
     i = idx[:, :DIM]
     j = idx[:, DIM:]
@@ -66,34 +95,8 @@ def alg_bytes(hg, info, npts, s_b):
     dims = np.broadcast_to(np.arange(DIM), i.shape)[nz].astype(np.int64)
     keys = (dims << 32) | (i[nz].astype(np.int64) << 16) | j[nz].astype(np.int64)
     szxps = int(np.unique(keys).size) + 1
-    return (npts * DIM * 8 + npts * TD * 8 + info.nno * TD * s_b + info.ncoarse * TD * 4
-            + 2 * info.nno * info.max_comps + 4 * szxps), szxps
-
-
-# Random 1 KB row gathers from an L2-resident region measured 18.2G rows/s
-# (18.7 TB/s) on this pool's B200s with 16-byte loads at 32 warps per SM
-# (profiles/gather_roof_probe.md): the roof of a kernel whose work is one row
-# gather per (point, active node) pair.
-GATHER_PEAK_TBS = 18.7
-
-# DRAM bytes (read + write) of one FP32C step of the default workload: the sum
-# over the 16 fwd_f32d_kernel launches (node chunks of 64,768) of one forward
-# call in an ncu capture (profiles/fwd_f32d_c4_traffic.md).
-FP32C_STEP_DRAM_BYTES = 48.9e9
-
-
-def gather_roof(mean_active, ms, grid, hg):
-    """Row bytes the FP32C step gathers (one FP32 row per active pair, a lower
-    bound) over the step time, against the measured gather peak."""
-    info = grid.info
-    row32 = info.ld * 4
-    bytes_per_pair = row32  # lower bound: every pair reads at least its FP32 row
-    b = mean_active * NPTS * bytes_per_pair
-    ach = b / (ms * 1e-3) / 1e12
-    return {"bound": "l2_gather", "achieved": ach, "peak": GATHER_PEAK_TBS, "unit": "TB/s",
-            "frac": ach / GATHER_PEAK_TBS, "bytes_per_pair": bytes_per_pair,
-            "note": "one FP32 row (TotalDof x 4 B) per active (point, node) pair over the step time; big "
-                    "terms read their FP64 row (2x) and dropped terms read none"}
+    rows = info.nno * TD * 4 + info.ncoarse * TD * 8 if fp32c else info.nno * TD * 8
+    return npts * DIM * 8 + npts * TD * 8 + rows + 2 * info.nno * info.max_comps + 4 * szxps, szxps
 
 
 class Clocks:
@@ -142,17 +145,67 @@ class Clocks:
                 "samples": len(rows)}
 
 
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def spawn_ranks(n):
+    """One process per GPU: re-run this command under torchrun with n ranks."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={free_port()}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def init_ranks(args, backend):
+    """Process group of the launched ranks; WORLD_SIZE must equal --gpus."""
+    import datetime
+    import torch.distributed as dist
+    rank, world, local = env_rank()
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    if world > 1:
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def max_over_ranks(values, world, device):
+    import torch
+    import torch.distributed as dist
+    if world == 1:
+        return list(values)
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def run_launch_check(args):
+    """The launcher, process group, barrier and max-over-ranks reduction of the
+    multi-GPU path on CPU (gloo), without any GPU work: every rank reports a
+    time of rank + 1 ms and rank 0 prints the maximum."""
+    import torch.distributed as dist
+    rank, world, _ = init_ranks(args, "gloo")
+    if world > 1:
+        dist.barrier()
+    (ms,) = max_over_ranks([rank + 1.0], world, "cpu")
+    if rank == 0:
+        print(json.dumps({"launch_check": "ok", "n_gpus": world, "max_over_ranks_ms": ms}))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_gpu(args):
+    import ctypes
     import torch
     import torch.distributed as dist
 
     import hddm_b200 as H
 
-    rank, world, local = env_rank()
+    rank, world, local = init_ranks(args, "nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     npts = args.points
     hg, X, t_gen = make_workload(npts=npts, seed_offset=rank)
     t0 = time.time()
@@ -170,7 +223,7 @@ def run_gpu(args):
         torch.cuda.synchronize(dev)
 
     def timed(plan, steps, warmup):
-        """Replays of the plan's CUDA graph (autotuned node chunks)."""
+        """Replays of the plan's CUDA graph; CUDA events on the replay stream."""
         for _ in range(warmup):
             plan.launch(stream=stream)
         barrier()
@@ -180,59 +233,20 @@ def run_gpu(args):
             plan.launch(stream=stream)
             ev[s + 1].record(stream)
         barrier()
-        per = [ev[s].elapsed_time(ev[s + 1]) for s in range(steps)]
-        total = ev[0].elapsed_time(ev[steps])
-        return total, per, plan.launches
-
-    if args.profile_replay:
-        # two FP32C forward calls (a warm-up and a measured one) with a fixed
-        # node-chunk size and kernel variant, nothing else: the case a
-        # launch-level capture looks at (skip the first call's launches)
-        chunk = args.chunk_rows if args.chunk_rows >= 0 else 64768
-        H.set_chunk_rows(chunk)
-        H.set_fp32c_variant(args.variant)
-        for _ in range(2):
-            H.interpolate(grid, x, precision=H.FP32C, out=out32, stream=stream)
-        torch.cuda.synchronize(dev)
-        print(json.dumps({"profile_replay": {"chunk_rows": chunk, "variant": args.variant,
-                                             "launches_per_call": H.last_launch().kernels}}))
-        return
-    # accuracy of the FP32C form against the FP64 form (bit-identical to gold), all points
-    H.interpolate(grid, x, precision=H.FP64, out=out64, stream=stream)
-    H.interpolate(grid, x, precision=H.FP32C, out=out32, stream=stream)
-    torch.cuda.synchronize(dev)
-    den = torch.maximum(out64.abs(), 1e-3 * out64.abs().amax(dim=1, keepdim=True))
-    perr = ((out32 - out64).abs() / den).amax(dim=1)
-    err_max, err_rms = float(perr.max()), float(perr.pow(2).mean().sqrt())
-    if args.only_accuracy_pass:
-        H.active_count(grid, x, stream=stream)
-        torch.cuda.synchronize(dev)
-        print(json.dumps({"fp32c_max_rel_err": err_max, "fp32c_rms_rel_err": err_rms, "points": npts}))
-        return
-    # the tree walk alone (hit counting, no accumulation) over every point
-    for _ in range(2):
-        counts = H.active_count(grid, x, stream=stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    counts = H.active_count(grid, x, stream=stream)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    walk_ms = e0.elapsed_time(e1)
-    mean_active = float(counts.double().mean())
+        return ev[0].elapsed_time(ev[steps])
 
     t_tune = time.time()
     plan32 = H.Plan(grid, x, out32, precision=H.FP32C, chunk_rows=args.chunk_rows, stream=stream)
     plan64 = H.Plan(grid, x, out64, precision=H.FP64, chunk_rows=args.chunk_rows, stream=stream)
     t_tune = time.time() - t_tune
     with Clocks(local) as clk:
-        t32, per32, k32 = timed(plan32, args.steps, args.warmup)
-        t64, per64, k64 = timed(plan64, args.steps, args.warmup)
+        t32 = timed(plan32, args.steps, args.warmup)
+        t64 = timed(plan64, args.steps, args.warmup)
     clocks = clk.summary()
 
     # end to end through the C ABI's host-pointer entry: pinned x in, pinned out back
     xh = torch.from_numpy(X).pin_memory()
     outh = torch.empty((npts, TD), dtype=torch.float64).pin_memory()
-    import ctypes
     offs = np.array([0, npts], np.int64)
     garr = (ctypes.c_void_p * 1)(grid.handle.value)
 
@@ -241,7 +255,7 @@ def run_gpu(args):
         if rc:
             raise H.SgiError(rc, H.lib.sgi_last_error().decode())
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(args.warmup):
         e2e_once()
     barrier()
     te = time.perf_counter()
@@ -250,26 +264,43 @@ def run_gpu(args):
     barrier()
     t_e2e = (time.perf_counter() - te) * 1e3
 
-    # max over ranks
-    def maxr(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    # untimed: the walk alone, and the terms per class (the bytes the FP32C
+    # kernels gather), over every point
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    H.active_count(grid, x, stream=stream)
+    e0.record(stream)
+    counts = H.active_count(grid, x, stream=stream)
+    e1.record(stream)
+    classes = H.term_classes(grid, x, stream=stream).sum(dim=0)
+    torch.cuda.synchronize(dev)
+    walk_ms = e0.elapsed_time(e1)
+    pairs = float(counts.double().sum())
+    n_big, n_fine, n_drop = (float(v) for v in classes.cpu())
+    o64_sub = o32_sub = None
+    if world == 1 and npts == NPTS:
+        sub = torch.from_numpy(check_subsample()).to(dev)
+        o64_sub = out64.index_select(0, sub).cpu().numpy()
+        o32_sub = out32.index_select(0, sub).cpu().numpy()
 
-    t32, t64, t_e2e = maxr(t32), maxr(t64), maxr(t_e2e)
+    t32, t64, t_e2e = max_over_ranks([t32, t64, t_e2e], world, dev)
     result = None
     if rank == 0:
         hbm, peak_kind = peaks()
-        b32, szxps = alg_bytes(hg, info, npts, 4)
-        b64, _ = alg_bytes(hg, info, npts, 8)
+        b32, szxps = alg_bytes(hg, info, npts, True)
         ms32 = t32 / args.steps
         ms64 = t64 / args.steps
-        ach = b32 / (ms32 * 1e-3) / 1e9
+        b64, _ = alg_bytes(hg, info, npts, False)
         pts_s = npts * world / (ms32 * 1e-3)
         pts64_s = npts * world / (ms64 * 1e-3)
-        traffic = FP32C_STEP_DRAM_BYTES if npts == NPTS else None
+        ach = b32 / (ms32 * 1e-3) / 1e9
+        gather_b = n_fine * info.ld * 4 + n_big * info.ld * 8
+        warps = VARIANT_WARPS.get(plan32.variant % 3, 32)
+        gpeak = GATHER_PEAK_TBS[64 if warps > 32 else 32]
+        gach = gather_b / (ms32 * 1e-3) / 1e12
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+        flops = 2.0 * pairs * TD
+        traffic = FP32C_CALL_DRAM_BYTES.get((plan32.chunk_rows, plan32.variant)) if npts == NPTS else None
         result = {
             "metric": METRIC,
             "value": pts_s,
@@ -282,40 +313,50 @@ def run_gpu(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32+comp (f64 in/out)",
-            "data": "synthetic: seeded adaptive grid and points (reference's large grids are not in its tree)",
+            "data": "synthetic: seeded adaptive grid and points (the reference's large grids are not in its tree)",
             "config": {"workload": WORKLOAD, "dim": DIM, "nno": info.nno, "TotalDof": TD, "points_per_gpu": npts,
                        "max_comps": info.max_comps, "ncoarse": info.ncoarse, "szxps": szxps,
-                       "mean_active_nodes_per_point": mean_active,
+                       "mean_active_nodes_per_point": pairs / npts,
                        "l2": "inputs larger than L2 (x 472 MB, surplus 1 GB FP32 / 2 GB FP64)",
                        "parallelism": f"replicated grid, points sharded, {world} GPU(s)"},
             "points_x_outputs_per_s": pts_s * TD,
             "fp64_form": {"points_per_s": pts64_s, "ms_per_step": ms64,
                           "roofline_frac": b64 / (ms64 * 1e-3) / 1e9 / hbm},
             "speedup_fp32c_vs_fp64_form": pts_s / pts64_s,
-            "fp32c_vs_gold_exact_fp64": {"max_rel_err": err_max, "rms_rel_err": err_rms, "points": npts},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                         "peak_kind": f"{peak_kind} (burst copy)", "algorithmic_bytes_per_launch": b32,
-                         "traffic": traffic, "kernel": "fwd_f32d_kernel",
-                         "traffic_note": "ncu DRAM read+write of one forward call with node chunks of 64,768 "
-                                         "(16 launches); the timed plan's chunking is in plans.fp32c"},
-            "gather_roofline": gather_roof(mean_active, ms32, grid, hg),
+                         "traffic": traffic, "peak_kind": f"{peak_kind} (burst copy)",
+                         "algorithmic_bytes_per_call": b32, "kernel": "fwd_f32d_kernel",
+                         "per": f"one forward call: one CUDA-graph replay of {plan32.launches} node-chunk launches",
+                         "traffic_note": "ncu DRAM read+write of one call with the plan's chunking "
+                                         "(null when that chunking was not captured)"},
+            "gather_roofline": {"bound": "l2_row_gather", "achieved": gach, "unit": "TB/s",
+                                "peak": gpeak, "frac": gach / gpeak, "peak_64_warps_per_sm": GATHER_PEAK_TBS[64],
+                                "frac_of_64_warp_peak": gach / GATHER_PEAK_TBS[64],
+                                "bytes_per_call": gather_b, "kernel_warps_per_sm": warps,
+                                "terms": {"big_fp64_rows": n_big, "fine_fp32_rows": n_fine, "dropped": n_drop},
+                                "note": "rows the FP32C kernel reads: fine terms x TotalDof x 4 B + big terms x "
+                                        "TotalDof x 8 B (dropped terms read none), over the step time; peak: random "
+                                        "1 KB row gathers from L2 at the kernel's warps per SM"},
+            "fma_work": {"active_pairs_per_call": pairs, "flops_per_call": flops,
+                         "achieved_tflops": flops / (ms32 * 1e-3) / 1e12,
+                         "fp32_peak_tflops": fp32_peak, "frac": flops / (ms32 * 1e-3) / 1e12 / fp32_peak,
+                         "note": "2 x TotalDof per active (point, node) pair; peak: nominal 148 SMs x 128 FP32 "
+                                 "lanes x 2 at the median SM clock sampled in the timed region"},
             "walk_only_ms": walk_ms,
-            "fma_work": {"mean_active_nodes": mean_active,
-                         "flops_per_launch": 2.0 * mean_active * TD * npts,
-                         "achieved_tflops": 2.0 * mean_active * TD * npts / (ms32 * 1e-3) / 1e12},
             "e2e": {"value": npts * world / (t_e2e / args.steps * 1e-3), "unit": "points/s",
                     "h2d_bytes_per_step": npts * DIM * 8, "d2h_bytes_per_step": npts * TD * 8},
-            "gpu_launches": args.steps * (k32 + k64),
+            "gpu_launches": args.steps * plan32.launches,
             "clocks": clocks,
             "setup_s": {"generate": round(t_gen, 2), "layout_and_upload": round(t_upload, 2),
                         "autotune_and_capture": round(t_tune, 2)},
             "plans": {"fp32c": {"chunk_rows": plan32.chunk_rows, "variant": plan32.variant,
                                 "launches": plan32.launches},
                       "fp64": {"chunk_rows": plan64.chunk_rows, "launches": plan64.launches},
-                      "note": "each step replays one CUDA graph holding all node-chunk launches"},
+                      "note": "each step replays one CUDA graph holding all node-chunk launches; gpu_launches "
+                              "counts the FP32C steps' kernels"},
         }
-    if rank == 0 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(hg, X, args.cpu_sample, args.cpu_variant)
+        if world == 1 and not args.no_cpu_baseline:
+            result.update(cpu_leg(hg, X, o64_sub, o32_sub, args.cpu_sample))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -323,33 +364,53 @@ def run_gpu(args):
         print(json.dumps(result))
 
 
-def cpu_baseline(hg, X, sample, variant):
-    """The reference's own CPU kernel (oracle/_ref) on a bounded sample of the
-    workload's points, one call per point, all host threads."""
+def cpu_leg(hg, X, o64_sub, o32_sub, sample):
+    """Host-side leg (rank 0, one GPU): the oracle checks the timed plans'
+    outputs on the 4,096-point subsample (FP64 bit for bit, FP32C relative
+    error), and the reference's own CPU kernel (oracle/_ref, avx2) is timed on
+    a bounded sample of the workload's points, one call per point, all host
+    threads."""
     import oracle as O
+    cores = os.cpu_count() or 1
+    res = {}
+    if o64_sub is not None:
+        sub = check_subsample()
+        ref = O.Gold(*hg.arrays()).interpolate(X[sub], nthreads=cores)
+        emax, erms = O.rel_error(o32_sub, ref)
+        res["parity_vs_oracle"] = {
+            "points": CHECK_POINTS, "subsample_seed": CHECK_SEED,
+            "fp64_bit_exact_vs_oracle": bool(np.array_equal(o64_sub, ref)),
+            "fp64_max_abs_diff": float(np.abs(o64_sub - ref).max()),
+            "fp32c_vs_oracle_gold": {"max_rel_err": emax, "rms_rel_err": erms},
+            "note": "outputs of the last timed replay of each plan against the oracle's gold restatement"}
+    variant = "avx2"
     if not O.ref_available(variant):
-        return {"value": None, "unit": "points/s", "kind": "reference", "cores": 0,
-                "sample": f"oracle/_ref/libref_{variant}.so not built"}
+        res["cpu_baseline"] = {"value": None, "unit": "points/s", "kind": "reference", "cores": 0,
+                               "sample": f"oracle/_ref/libref_{variant}.so not built"}
+        return res
     with tempfile.TemporaryDirectory() as td:
         p = os.path.join(td, "grid.plt")
         hg.write_plt(p)
         t = time.time()
         r = O.RefGrid(p, DIM, variant)
         t_load = time.time() - t
-        cores = os.cpu_count() or 1
         half = len(X) // 2
-        sub = np.ascontiguousarray(np.concatenate([X[:sample // 2], X[half:half + sample - sample // 2]]))
-        r.interpolate(sub[:cores], nthreads=cores)
+        pts = np.ascontiguousarray(np.concatenate([X[:sample // 2], X[half:half + sample - sample // 2]]))
+        r.interpolate(pts[:cores], nthreads=cores)
         t = time.perf_counter()
-        r.interpolate(sub, nthreads=cores)
+        r.interpolate(pts, nthreads=cores)
         dt = time.perf_counter() - t
-    return {"value": len(sub) / dt, "unit": "points/s", "kind": "reference", "cores": cores,
-            "variant": variant, "load_s": round(t_load, 1),
-            "sample": f"{len(sub)} of the workload's points (half uniform, half clustered), "
-                      f"LinearBasis_{variant}_Generic_InterpolateArray per point, {cores} threads"}
+    res["cpu_baseline"] = {"value": len(pts) / dt, "unit": "points/s", "kind": "reference", "cores": cores,
+                           "variant": variant, "load_s": round(t_load, 1),
+                           "sample": f"{len(pts)} of the workload's points (half uniform, half clustered), "
+                                     f"LinearBasis_{variant}_Generic_InterpolateArray per point, {cores} threads"}
+    return res
 
 
 def run_reference(args):
+    """The reference's own CPU kernel over a bounded sample of the workload per
+    step; the grid file and the points come from the oracle's generator (the
+    product library is not loaded)."""
     rank, world, _ = env_rank()
     if rank != 0:
         return
@@ -359,35 +420,37 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/libref_{variant}.so not built "
                           "(needs the reference tree at build time)"}))
         return
-    hg, X, _ = make_workload()
     cores = os.cpu_count() or 1
+    og = O.Gold.adaptive(DIM, NNO, TD, GRID_SEED)
+    X = O.gen_points(DIM, NPTS, 2, POINT_SEED)
     with tempfile.TemporaryDirectory() as td:
         p = os.path.join(td, "grid.plt")
-        hg.write_plt(p)
+        og.write_plt(p)
+        del og
         r = O.RefGrid(p, DIM, variant)
         rng = np.random.default_rng(0)
         times = []
         for s in range(args.warmup + args.steps):
-            sub = X[rng.choice(NPTS, args.cpu_sample, replace=False)]
+            sub = X[rng.choice(NPTS, args.ref_sample, replace=False)]
             t = time.perf_counter()
             r.interpolate(sub, nthreads=cores)
             if s >= args.warmup:
                 times.append(time.perf_counter() - t)
     ms = float(np.mean(times)) * 1e3
-    v = args.cpu_sample / (ms * 1e-3)
+    v = args.ref_sample / (ms * 1e-3)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (same grid and points)",
-        "config": {"workload": WORKLOAD, "sample_points_per_step": args.cpu_sample},
+        "config": {"workload": WORKLOAD, "sample_points_per_step": args.ref_sample},
         "cpu_baseline": {"value": v, "unit": "points/s", "kind": "reference", "cores": cores,
-                         "sample": f"{args.cpu_sample} random points of the workload per step, "
+                         "sample": f"{args.ref_sample} random points of the workload per step, "
                                    f"LinearBasis_{variant}_Generic_InterpolateArray, {cores} threads"},
         "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
-def _plan_time(H, torch, plan, stream, steps, warmup):
+def _plan_time(torch, plan, stream, steps, warmup):
     for _ in range(warmup):
         plan.launch(stream=stream)
     torch.cuda.synchronize()
@@ -398,12 +461,6 @@ def _plan_time(H, torch, plan, stream, steps, warmup):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / steps
-
-
-def _rel_err(torch, a, b):
-    den = torch.maximum(b.abs(), 1e-3 * b.abs().amax(dim=1, keepdim=True))
-    e = ((a - b).abs() / den).amax(dim=1)
-    return float(e.max()), float(e.pow(2).mean().sqrt())
 
 
 def run_c2(args):
@@ -424,72 +481,14 @@ def run_c2(args):
     o64 = torch.empty_like(o32)
     p32 = H.Plan(grids, x, o32, counts=list(counts), precision=H.FP32C, stream=stream)
     p64 = H.Plan(grids, x, o64, counts=list(counts), precision=H.FP64, stream=stream)
-    ms32 = _plan_time(H, torch, p32, stream, args.steps, args.warmup)
-    ms64 = _plan_time(H, torch, p64, stream, args.steps, args.warmup)
-    emax, erms = _rel_err(torch, o32, o64)
+    ms32 = _plan_time(torch, p32, stream, args.steps, args.warmup)
+    ms64 = _plan_time(torch, p64, stream, args.steps, args.warmup)
     npts = int(counts.sum())
     print(json.dumps({"workload": "C2: 8 multistate grids d=30, TotalDof=64, ragged batches", "grids_nno": nnos.tolist(),
                       "points_per_grid": counts.tolist(), "points": npts,
                       "fp32c": {"ms": ms32, "points_per_s": npts / ms32 * 1e3, "variant": p32.variant,
                                 "chunk_rows": p32.chunk_rows, "launches": p32.launches},
-                      "fp64": {"ms": ms64, "points_per_s": npts / ms64 * 1e3, "launches": p64.launches},
-                      "fp32c_vs_gold_exact_fp64": {"max_rel_err": emax, "rms_rel_err": erms}}))
-
-
-def run_chunksweep(args):
-    """Step time of both forms over fixed node-chunk sizes (the autotuner's
-    search space, printed), default workload."""
-    import torch
-    import hddm_b200 as H
-    dev = torch.device("cuda", 0)
-    hg, X, _ = make_workload(npts=args.points)
-    g = H.Grid(hg, flags=H.BUILD_FP32)
-    x = torch.from_numpy(X).to(dev)
-    out = torch.empty((X.shape[0], TD), dtype=torch.float64, device=dev)
-    s = torch.cuda.current_stream(dev)
-    rows_list = [0, 16384, 32768, 49152, 65536, 98304, 131072, 196608, 262144]
-    res = {}
-    for prec, name in ((H.FP32C, "fp32c"), (H.FP64, "fp64")):
-        for rows in rows_list:
-            p = H.Plan(g, x, out, precision=prec, chunk_rows=rows, stream=s)
-            res.setdefault(name, []).append({"chunk_rows": rows, "launches": p.launches,
-                                             "ms": _plan_time(H, torch, p, s, 3, 2)})
-            del p
-    print(json.dumps({"workload": WORKLOAD, "chunk_sweep": res}))
-
-
-def run_variantsweep(args):
-    """FP32C step time of every kernel variant over node-chunk sizes (direct
-    calls, CUDA events), with each variant's error against the gold-exact FP64
-    form, default workload."""
-    import torch
-    import hddm_b200 as H
-    dev = torch.device("cuda", 0)
-    hg, X, _ = make_workload(npts=args.points)
-    g = H.Grid(hg, flags=H.BUILD_FP32)
-    x = torch.from_numpy(X).to(dev)
-    ref = H.interpolate(g, x, precision=H.FP64)
-    rows_list = [int(r) for r in args.sweep_rows.split(",")]
-    res = []
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for v in [int(k) for k in args.sweep_variants.split(",")]:
-        H.set_fp32c_variant(v)
-        for rows in rows_list:
-            H.set_chunk_rows(rows)
-            out = H.interpolate(g, x, precision=H.FP32C)
-            torch.cuda.synchronize()
-            e0.record()
-            for _ in range(3):
-                H.interpolate(g, x, precision=H.FP32C, out=out)
-            e1.record()
-            torch.cuda.synchronize()
-            emax, erms = _rel_err(torch, out, ref)
-            res.append({"variant": v, "chunk_rows": rows, "ms": e0.elapsed_time(e1) / 3,
-                        "max_rel_err": emax, "rms_rel_err": erms})
-            print(json.dumps(res[-1]), file=sys.stderr)
-    H.set_fp32c_variant(-1)
-    H.set_chunk_rows(-1)
-    print(json.dumps({"workload": WORKLOAD, "variant_sweep": res}))
+                      "fp64": {"ms": ms64, "points_per_s": npts / ms64 * 1e3, "launches": p64.launches}}))
 
 
 def run_c3(args):
@@ -510,7 +509,7 @@ def run_c3(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
-        gx, gs = H.backward(g, x, c)
+        H.backward(g, x, c)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
@@ -521,56 +520,14 @@ def run_c3(args):
     torch.cuda.synchronize()
     fms = e0.elapsed_time(e1) / args.steps
     pairs = float(H.active_count(g, x).double().sum())
+    # bytes the backward must move at least: coordinates, dL/dvalue and dL/dx
+    # per point, one FP64 surplus row read and one dL/dsurplus row written per node
+    b_alg = 32768 * (59 * 8 * 2 + 128 * 8) + hg.nno * 128 * 8 * 2
     print(json.dumps({"workload": "C3: backward, d=59, 300k nodes, TotalDof=128, 32768 points",
                       "backward_ms": ms, "forward_fp64_ms": fms, "active_pairs": pairs,
                       "backward_points_per_s": 32768 / ms * 1e3,
-                      "grad_norms": {"dx": float(gx.norm()), "dsurplus": float(gs.norm())}}))
-
-
-def run_errors(args):
-    """FP32C max / RMS relative error against the FP64 form (bit-identical to the
-    reference's gold path, as the GPU tests check), and both forms' step times
-    (graph-plan replays), on every config's inputs:
-    C0 regular d=4 level 4, TotalDof 8, 1024 points; C1 regular d=16 level 5,
-    TotalDof 32, 65,536 points; C2 eight adaptive d=30 grids, TotalDof 64,
-    ragged batches; C3 adaptive d=59, 300k nodes, TotalDof 128, 32,768
-    points; C4 the benchmark workload."""
-    import torch
-    import hddm_b200 as H
-    dev = torch.device("cuda", 0)
-
-    stream = torch.cuda.current_stream(dev)
-
-    def errs(grids, X, counts=None):
-        x = torch.from_numpy(X).to(dev)
-        o64 = H.interpolate(grids, x, counts=counts, precision=H.FP64)
-        o32 = H.interpolate(grids, x, counts=counts, precision=H.FP32C)
-        emax, erms = _rel_err(torch, o32, o64)
-        # step times of autotuned graph plans of both forms (CUDA events)
-        p64 = H.Plan(grids, x, o64, counts=counts, precision=H.FP64, stream=stream)
-        p32 = H.Plan(grids, x, o32, counts=counts, precision=H.FP32C, stream=stream)
-        ms64 = _plan_time(H, torch, p64, stream, max(args.steps, 5), args.warmup)
-        ms32 = _plan_time(H, torch, p32, stream, max(args.steps, 5), args.warmup)
-        return {"points": len(X), "max_rel_err": emax, "rms_rel_err": erms,
-                "fp64_ms": ms64, "fp32c_ms": ms32, "fp32c_points_per_s": len(X) / ms32 * 1e3}
-
-    res = {}
-    g0 = H.HostGrid.regular(4, 4, 8, seed=0)
-    res["C0"] = dict(nno=g0.nno, **errs(H.Grid(g0, flags=H.BUILD_FP32), H.gen_points(4, 1024, kind=0, seed=0)))
-    g1 = H.HostGrid.regular(16, 5, 32, seed=1)
-    res["C1"] = dict(nno=g1.nno, **errs(H.Grid(g1, flags=H.BUILD_FP32), H.gen_points(16, 65536, kind=0, seed=1)))
-    rng = np.random.Generator(np.random.PCG64(2))
-    nnos = np.exp(rng.uniform(np.log(20_000), np.log(200_000), 8)).astype(int)
-    counts = rng.integers(1, 100_001, 8)
-    grids = [H.Grid(H.HostGrid.adaptive(30, int(n), 64, seed=200 + k), flags=H.BUILD_FP32) for k, n in enumerate(nnos)]
-    res["C2"] = dict(nno=nnos.tolist(), **errs(grids, H.gen_points(30, int(counts.sum()), kind=0, seed=2), list(counts)))
-    del grids
-    g3 = H.HostGrid.adaptive(59, 300_000, 128, seed=3)
-    res["C3"] = dict(nno=g3.nno, **errs(H.Grid(g3, flags=H.BUILD_FP32),
-                                         H.gen_points(59, 32768, kind=0, seed=3, kink_reject=1e-6)))
-    hg, X, _ = make_workload()
-    res["C4"] = dict(nno=hg.nno, **errs(H.Grid(hg, flags=H.BUILD_FP32), X))
-    print(json.dumps({"fp32c_vs_gold_exact_fp64": res}))
+                      "algorithmic_bytes": b_alg, "pair_row_bytes": pairs * 128 * 8 * 2,
+                      "pair_row_tbs": pairs * 128 * 8 * 2 / (ms * 1e-3) / 1e12}))
 
 
 def run_multistate(args):
@@ -595,7 +552,6 @@ def run_multistate(args):
     for _ in range(reps):
         rc = H.lib.sgi_interpolate_host(ns, arr, offs.ctypes.data, xh.ctypes.data, outh.ctypes.data, H.FP64)
     host_s = (time.perf_counter() - t) / reps
-    # one point on the first state, both forms
     single = {}
     off1 = np.array([0, 1], np.int64)
     for name, prec in (("fp64", H.FP64), ("fp32c", H.FP32C)):
@@ -609,7 +565,7 @@ def run_multistate(args):
     out = torch.empty((ns, 118), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
     plan = H.Plan(grids, x, out, counts=[1] * ns, precision=H.FP64, chunk_rows=0, stream=stream)
-    dev_ms = _plan_time(H, torch, plan, stream, reps, args.warmup)
+    dev_ms = _plan_time(torch, plan, stream, reps, args.warmup)
     print(json.dumps({"workload": "multistate call: 16 states x 1 point, d=59, TotalDof=118, 200k nodes per state",
                       "rc": rc, "host_call_s": host_s, "host_s_per_state": host_s / ns,
                       "graph_replay_ms": dev_ms, "graph_s_per_state": dev_ms * 1e-3 / ns,
@@ -618,75 +574,39 @@ def run_multistate(args):
                                                           "large, avx2 (daint)": 4.234e-3}}))
 
 
-def run_cutoffsweep(args):
-    """FP32C step time (graph replay) and error against the gold-exact FP64 form
-    for surplus cutoffs of 2^-k of the largest |surplus|, default workload."""
-    import torch
-    import hddm_b200 as H
-    dev = torch.device("cuda", 0)
-    hg, X, _ = make_workload(npts=args.points)
-    g = H.Grid(hg, flags=H.BUILD_FP32)
-    x = torch.from_numpy(X).to(dev)
-    ref = H.interpolate(g, x, precision=H.FP64)
-    smax = g.set_surplus_cutoff(0.0) * 2.0 ** 46
-    stream = torch.cuda.Stream(dev)
-    res = []
-    for k in [int(v) for v in args.sweep_cutoffs.split(",")]:
-        eff = g.set_surplus_cutoff(smax * 2.0 ** -k)
-        out = torch.empty(x.shape[0], TD, dtype=torch.float64, device=dev)
-        plan = H.Plan(g, x, out, precision=H.FP32C, chunk_rows=args.chunk_rows, stream=stream)
-        ms = _plan_time(H, torch, plan, stream, 5, 3)
-        emax, erms = _rel_err(torch, out, ref)
-        res.append({"cutoff_log2_of_max_surplus": -k, "cutoff": eff, "ms": ms, "max_rel_err": emax,
-                    "rms_rel_err": erms, "chunk_rows": plan.chunk_rows, "variant": plan.variant})
-        print(json.dumps(res[-1]), file=sys.stderr)
-        del plan
-    g.set_surplus_cutoff(0.0)
-    print(json.dumps({"workload": WORKLOAD, "cutoff_sweep": res}))
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "chunksweep", "variantsweep", "errors",
-                                                        "cutoffsweep"],
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate"],
                     help="c4 (default) is the benchmark line; the others print their own measurements")
-    ap.add_argument("--cpu-sample", type=int, default=256)
-    ap.add_argument("--sweep-variants", default="0,1,2", help="variantsweep: FP32C variants")
-    ap.add_argument("--sweep-rows", default="0,131072,196608,262144,393216", help="variantsweep: chunk sizes")
-    ap.add_argument("--sweep-cutoffs", default="46,40,36,34,32,30",
-                    help="cutoffsweep: k of the cutoffs 2^-k * max|surplus| (46 is the default bound)")
+    ap.add_argument("--cpu-sample", type=int, default=16384,
+                    help="points of the CPU baseline's timed sample (default: 16,384)")
+    ap.add_argument("--ref-sample", type=int, default=2048, help="--impl reference: points per step")
     ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the host leg (oracle check of the outputs and the CPU baseline)")
     ap.add_argument("--points", type=int, default=NPTS, help="points per GPU (default: the workload's 1M)")
     ap.add_argument("--chunk-rows", type=int, default=-1, help="node-chunk size of the plans (-1: autotune)")
-    ap.add_argument("--variant", type=int, default=1, help="--profile-replay: FP32C kernel variant")
-    ap.add_argument("--profile-replay", action="store_true",
-                    help="only run two replays of the FP32C plan (launch-level profiling case)")
-    ap.add_argument("--only-accuracy-pass", action="store_true",
-                    help="run one FP64 and one FP32C launch, print their agreement and exit (profiling case)")
+    ap.add_argument("--launch-check", action="store_true",
+                    help="check the multi-rank launcher and the max-over-ranks reduction on CPU (gloo), no GPU work")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "b200":
+        sys.exit(spawn_ranks(args.gpus))
+    if args.launch_check:
+        run_launch_check(args)
+    elif args.impl == "reference":
         run_reference(args)
-    elif args.workload == "errors":
-        run_errors(args)
     elif args.workload == "c2":
         run_c2(args)
     elif args.workload == "c3":
         run_c3(args)
     elif args.workload == "multistate":
         run_multistate(args)
-    elif args.workload == "chunksweep":
-        run_chunksweep(args)
-    elif args.workload == "variantsweep":
-        run_variantsweep(args)
-    elif args.workload == "cutoffsweep":
-        run_cutoffsweep(args)
     else:
         run_gpu(args)
 

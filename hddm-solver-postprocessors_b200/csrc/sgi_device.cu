@@ -1339,8 +1339,12 @@ __global__ void __launch_bounds__(LBLOCK) fwd_f64_list_kernel(const __grid_const
 	}
 }
 
-// Active-node count per point (single grid).
-__global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ FwdArgs a, long long* counts)
+// Active-node count per point (single grid).  With `classes` (a grid
+// descriptor of the FP32C form), also the point's terms by the FP32C form's
+// classes: classes[3p] big (FP64 row), [3p + 1] fine (FP32 row), [3p + 2]
+// dropped, by the bound |w| * max|s_row| of the full-product weight.
+__global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ FwdArgs a, long long* counts,
+	long long* classes)
 {
 	extern __shared__ double smem[];
 	const int lane = threadIdx.x & 31;
@@ -1352,10 +1356,31 @@ __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ Fw
 		p = __shfl_sync(FULL, p, 0);
 		if (p >= a.npts) break;
 		const GridDesc& G = a.g[find_grid(a, p)];
-		long long cnt = 0;
+		long long cnt = 0, nbig = 0, nfine = 0;
 		if (load_point(a, p, xs, lane))
-			traverse(G, xs, lane, [&](unsigned mask, int, double, const uint4&, float) { cnt += __popc(mask); });
-		if (lane == 0) counts[p] = cnt;
+			traverse(G, xs, lane, [&](unsigned mask, int, double w, const uint4& r, float rm)
+			{
+				cnt += __popc(mask);
+				if (classes)
+				{
+					const bool hit = (mask >> lane) & 1u;
+					const float bound = fabsf(__double2float_rn(w)) * rm;
+					const bool big = hit && (r.z & NODE_COARSE) && bound >= G.big_below;
+					const bool fine = hit && !big && bound >= G.skip_below;
+					nbig += __popc(__ballot_sync(FULL, big));
+					nfine += __popc(__ballot_sync(FULL, fine));
+				}
+			});
+		if (lane == 0)
+		{
+			if (counts) counts[p] = cnt;
+			if (classes)
+			{
+				classes[3 * p] = nbig;
+				classes[3 * p + 1] = nfine;
+				classes[3 * p + 2] = cnt - nbig - nfine;
+			}
+		}
 		__syncwarp();
 	}
 }
@@ -2469,18 +2494,17 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 	return SGI_OK;
 }
 
-extern "C" int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream)
+namespace {
+
+int count_terms(sgi_grid_t g, long long npts, const double* x, long long* counts, long long* classes, void* stream)
 {
-	clear_error();
-	if (!g || npts < 0 || (npts && (!x || !out))) return fail(SGI_E_INVALID, "bad arguments");
-	if (!npts) return SGI_OK;
 	DeviceGuard guard(g->device);
 	DeviceWork* W = nullptr;
 	int rc = device_work(g->device, &W);
 	if (rc) return rc;
 	FwdArgs a;
 	memset(&a, 0, sizeof(a));
-	a.g[0] = desc_of(g, 0);
+	a.g[0] = desc_of(g, 0, classes ? SGI_FP32C : SGI_FP64);
 	a.x = x; a.npts = npts; a.ngrids = 1; a.dim = g->dim; a.TD = g->TD;
 	a.counter = W->counters + (W->next.fetch_add(1) % NCOUNTERS);
 	cudaStream_t s = (cudaStream_t)stream;
@@ -2490,9 +2514,28 @@ extern "C" int sgi_active_count(sgi_grid_t g, long long npts, const double* x, l
 	int blocks = 0;
 	rc = occupancy_grid(count_kernel, smem, W->sms, &blocks);
 	if (rc) return rc;
-	count_kernel<<<blocks, BLOCK, smem, s>>>(a, out);
+	count_kernel<<<blocks, BLOCK, smem, s>>>(a, counts, classes);
 	CUDA_TRY(cudaGetLastError());
 	return SGI_OK;
+}
+
+} // namespace
+
+extern "C" int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream)
+{
+	clear_error();
+	if (!g || npts < 0 || (npts && (!x || !out))) return fail(SGI_E_INVALID, "bad arguments");
+	if (!npts) return SGI_OK;
+	return count_terms(g, npts, x, out, nullptr, stream);
+}
+
+extern "C" int sgi_term_classes(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream)
+{
+	clear_error();
+	if (!g || npts < 0 || (npts && (!x || !out))) return fail(SGI_E_INVALID, "bad arguments");
+	if (!g->s32) return fail(SGI_E_INVALID, "term classes: the grid has no FP32 form (build with SGI_BUILD_FP32)");
+	if (!npts) return SGI_OK;
+	return count_terms(g, npts, x, nullptr, out, stream);
 }
 
 extern "C" int sgi_backward(sgi_grid_t g, long long npts, const double* x, const double* gout,

@@ -74,6 +74,7 @@ def _load():
         "sgi_interpolate_host": (I, [I, P, P, P, P, I]),
         "sgi_backward": (I, [P, LL, P, P, P, P, P]),
         "sgi_active_count": (I, [P, LL, P, P, P]),
+        "sgi_term_classes": (I, [P, LL, P, P, P]),
         "sgi_last_launch": (I, [ctypes.POINTER(LaunchStats)]),
         "sgi_set_chunk_rows": (I, [I]),
         "sgi_set_fp32c_variant": (I, [I]),
@@ -324,6 +325,14 @@ def active_count(grid, x, stream=None):
     import torch
     out = torch.empty(x.shape[0], dtype=torch.int64, device=x.device)
     _check(lib.sgi_active_count(grid.handle, x.shape[0], x.data_ptr(), out.data_ptr(), _stream_ptr(stream)))
+    return out
+
+
+def term_classes(grid, x, stream=None):
+    """FP32C terms per point by class: int64 [npts, 3] = (big, fine, dropped)."""
+    import torch
+    out = torch.empty((x.shape[0], 3), dtype=torch.int64, device=x.device)
+    _check(lib.sgi_term_classes(grid.handle, x.shape[0], x.data_ptr(), out.data_ptr(), _stream_ptr(stream)))
     return out
 
 

@@ -212,35 +212,50 @@ int sgi_backward(sgi_grid_t g, long long npts, const double* x, const double* go
  *
  * For callers that must not allocate device memory: a host solver that hands
  * all device memory to its own pre-reserved arena (an extra cudaMalloc can
- * fail or fragment it), code whose first call already runs inside CUDA stream
- * capture (cudaMalloc is not permitted while a stream is capturing), and
- * time-stepping loops that cannot afford cudaMalloc's implicit device
- * synchronization.  sgi_interpolate's work counters live in a workspace that
- * its first call on a device allocates; this variant instead keeps them in a
- * fixed array inside the library's device image, SGI_NOALLOC_MAX_LAUNCHES
- * counters of 8 bytes per device, held by every GPU that loads the library
- * until the process exits.
+ * fail or fragment it), and time-stepping loops that cannot afford
+ * cudaMalloc's implicit device synchronization.  sgi_interpolate's work
+ * counters live in a workspace that its first call on a device allocates;
+ * this variant instead keeps them in a fixed array inside the library's device
+ * image, SGI_NOALLOC_MAX_LAUNCHES counters of 8 bytes per device, held by
+ * every GPU that loads the library until the process exits.
  *
  * Arguments and results are those of sgi_interpolate (device x and out, host
- * pt_offsets); FP64 results are bit-identical to it.  Small batches run the
- * one-phase kernels here (sgi_interpolate's two-phase ones need scratch), so
- * small FP32C batches may differ from sgi_interpolate's in the last bits
- * (both within the FP32C tolerance).  A call makes ceil(ngrids / 48) * ceil(TotalDof / 256) kernel
- * launches (groups of grids with no points are skipped); a call that would need
- * more than SGI_NOALLOC_MAX_LAUNCHES launches is rejected with SGI_E_RANGE
- * before anything is launched.  The first call on each device looks up the
- * array's device address with that device current; make that first call before
- * any stream capture.  Every call shares the one array and clears the counters
- * it uses on `stream` before each launch, so calls that overlap on the GPU
- * (different streams, or different host threads) race on the counters and must
- * be serialized by the caller.  The call allocates nothing, neither itself nor
- * through CUDA or any library. */
+ * pt_offsets); FP64 results are bit-identical to it.  It launches every grid
+ * whole, never in node chunks (each chunk launch would take one more counter
+ * from the fixed array): on grids whose surplus rows exceed the L2, which
+ * sgi_interpolate walks in chunks for batches of 4096 points or more, it
+ * reads rows from HBM instead of the L2 and is slower, and its FP32C results
+ * may differ from sgi_interpolate's in the last bits (the order of the FP64
+ * additions differs; both stay within the FP32C tolerance).  Small batches
+ * run the one-phase kernels here (sgi_interpolate's two-phase ones need
+ * scratch), with the same consequence for FP32C bits.  A call makes
+ * ceil(ngrids / 48) * ceil(TotalDof / 256) kernel launches (groups of grids
+ * with no points are skipped); a call that would need more than
+ * SGI_NOALLOC_MAX_LAUNCHES launches is rejected with SGI_E_RANGE before
+ * anything is launched.  The first call on each device looks up the array's
+ * device address with that device current; make that first call before any
+ * stream capture.  Every call shares the one array and clears the counters it
+ * uses on `stream` before each launch, so calls that overlap on the GPU
+ * (different streams, or different host threads) race on the counters and
+ * must be serialized by the caller.  The call allocates nothing, neither
+ * itself nor through CUDA or any library. */
 #define SGI_NOALLOC_MAX_LAUNCHES 64
 int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
 	const double* x, double* out, int precision, void* stream);
 
 /* Active-node count A(x) per point (device int64 out[npts]); diagnostics. */
 int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream);
+
+/* The FP32C form's terms per point by class (device int64 out[3 * npts]):
+ * out[3p] big terms (rows with an FP64 copy whose bound |w| * max|s_row|
+ * reaches the coarse threshold: FP64 row reads), out[3p + 1] fine terms (FP32
+ * row reads), out[3p + 2] terms dropped unread (bound below the grid's
+ * negligible-term bound or surplus cutoff).  Bounds use the full-product
+ * weight rounded to FP32; the forward kernels build weights incrementally, so
+ * a term within rounding of a threshold may fall on the other side there.
+ * Diagnostics (the bytes the forward gathers); SGI_E_INVALID for a grid
+ * built without SGI_BUILD_FP32.  No reference counterpart. */
+int sgi_term_classes(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream);
 
 /* Node-range chunking of the forward launches (process-wide).  A grid whose
  * surplus rows exceed the L2 is walked in chunks of consecutive nodes (rows

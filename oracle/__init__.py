@@ -43,6 +43,11 @@ def lib():
         L.oracle_gradient.argtypes = [ctypes.POINTER(OracleGrid), ctypes.c_long, P, P, P, P]
         L.oracle_active_count.argtypes = [ctypes.POINTER(OracleGrid), P]
         L.oracle_active_count.restype = ctypes.c_long
+        L.oracle_gen_adaptive.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_ulonglong, ctypes.POINTER(OracleGrid)]
+        L.oracle_gen_points.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_int, ctypes.c_ulonglong,
+                                        ctypes.c_double, ctypes.c_int, P]
+        L.oracle_plt_write.argtypes = [ctypes.POINTER(OracleGrid), ctypes.c_char_p]
         _lib = L
     return _lib
 
@@ -97,9 +102,37 @@ class Gold:
                               ds.ctypes.data)
         return dx, ds
 
+    @classmethod
+    def adaptive(cls, dim, nno, total_dof, seed, max_level=7, p_dim=0.125):
+        """The seeded adaptive grid, generated by the oracle's restatement
+        (the same arrays as the product's generator)."""
+        g = OracleGrid()
+        if lib().oracle_gen_adaptive(dim, nno, total_dof, max_level, p_dim, seed, ctypes.byref(g)):
+            raise ValueError("bad adaptive-grid arguments")
+        index = np.ctypeslib.as_array(g.index, shape=(g.nno, 2 * g.dim)).copy()
+        surplus = np.ctypeslib.as_array(g.surplus, shape=(g.nno, g.TotalDof)).copy()
+        level = g.Level
+        lib().oracle_grid_free(ctypes.byref(g))
+        out = cls(index, surplus)
+        out.g.Level = level
+        return out
+
+    def write_plt(self, path):
+        """The compressed .plt layout the reference's loaders read."""
+        if lib().oracle_plt_write(ctypes.byref(self.g), os.fsencode(path)):
+            raise OSError(f"cannot write {path}")
+
     def active_count(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
         return lib().oracle_active_count(ctypes.byref(self.g), x.ctypes.data)
+
+
+def gen_points(dim, npts, kind=0, seed=0, kink_reject=0.0, max_level=7):
+    """The seeded query points, generated by the oracle's restatement."""
+    out = np.zeros((npts, dim), np.float64)
+    if lib().oracle_gen_points(dim, npts, kind, seed, kink_reject, max_level, out.ctypes.data):
+        raise ValueError("bad point arguments")
+    return out
 
 
 def ref_available(variant="gold"):

@@ -55,6 +55,17 @@ void oracle_gradient(const oracle_grid* g, long npts, const double* X, const dou
 /* Number of nodes with non-zero weight at x (the "active" count A(x)). */
 long oracle_active_count(const oracle_grid* g, const double* x);
 
+/* The seeded synthetic workload, restated (oracle/gen.c): the same grids and
+ * points as the product's sgi_gen_adaptive and sgi_gen_points.  The grid's
+ * arrays are malloc'd (free with oracle_grid_free).  Return 0 on success. */
+int oracle_gen_adaptive(int dim, int nno, int TotalDof, int max_level, double p_dim, unsigned long long seed,
+	oracle_grid* g);
+int oracle_gen_points(int dim, long npts, int kind, unsigned long long seed, double kink_reject, int max_level,
+	double* out);
+
+/* Writes the compressed .plt layout the reference's loaders read. */
+int oracle_plt_write(const oracle_grid* g, const char* path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,7 +4,7 @@
 // the timed CPU baseline, never part of the product.
 //
 // One copy of this file is compiled per reference variant (NAMESPACE = gold,
-// x86, avx2).  It provides what the missing parent project would provide:
+// x86, avx2, avx512).  It provides what the missing parent project would provide:
 //   * MPI_Process (declared at include/process.h:8-28) printing to stdio,
 //   * Interpolator::getInstance/getParameters (include/interpolator.h:18-42)
 //     with Parameters (LinearBasis/cpu/include/parameters.h) bound to globals,
@@ -25,6 +25,9 @@
 
 #include "interpolator.h"
 #include "Data.h"
+#if defined(ORACLE_REF_AVX512)
+#include "Device.h"
+#endif
 
 // ---------------------------------------------------------------- MPI_Process
 MPI_Process* MPI_Process::GoogleTest(int, char**) { return nullptr; }
@@ -72,7 +75,18 @@ Interpolator* Interpolator::getInstance()
 	return &instance;
 }
 
+#if defined(ORACLE_REF_AVX512)
+// Friend of Device (LinearBasis/avx512/include/Device.h): the avx512 kernel
+// sizes its per-thread scratch by the device's thread count, which the
+// parent's Devices sets; one thread here.
+class Devices
+{
+public :
+	static void serial(Device& d) { d.nthreads = 1; }
+};
+#else
 class Device;
+#endif
 
 // Friend of DataDense/DataSparse: read-only accessors for the loaded state.
 class GoogleTest
@@ -220,6 +234,13 @@ void ref_interpolate_batch(void* hv, int istate, long npts, const double* X, dou
 	std::atomic<long> next(0);
 	auto worker = [&]()
 	{
+#if defined(ORACLE_REF_AVX512)
+		Device dev;
+		Devices::serial(dev);
+		Device* device = &dev;
+#else
+		Device* device = nullptr;
+#endif
 		double* xbuf = (double*)aligned_alloc(64, sizeof(double) * ((dim + 15) / 16 * 16));
 		double* vbuf = (double*)aligned_alloc(64, sizeof(double) * TDpad);
 		memset(vbuf, 0, sizeof(double) * TDpad);
@@ -231,11 +252,14 @@ void ref_interpolate_batch(void* hv, int istate, long npts, const double* X, dou
 			for (long p = p0; p < p1; p++)
 			{
 				memcpy(xbuf, X + (size_t)p * dim, sizeof(double) * dim);
+#if defined(ORACLE_REF_AVX512)
+				memset(vbuf, 0, sizeof(double) * TDpad);   // the kernel adds into value
+#endif
 #if defined(ORACLE_REF_GOLD)
-				KERNEL_SINGLE(nullptr, dim, TD, xbuf, &RefAccess::index(d, istate),
+				KERNEL_SINGLE(device, dim, TD, xbuf, &RefAccess::index(d, istate),
 					&RefAccess::surplus(d, istate), vbuf);
 #else
-				KERNEL_SINGLE(nullptr, dim, TD, xbuf, RefAccess::nfreqs(d, istate),
+				KERNEL_SINGLE(device, dim, TD, xbuf, RefAccess::nfreqs(d, istate),
 					&RefAccess::xps(d, istate), &RefAccess::chains(d, istate),
 					&RefAccess::surplus(d, istate), vbuf);
 #endif

@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures under tests/golden/ from the reference tree.
 
 Run in a container that has the reference checked out (default
-/root/reference, override with --ref) after `make -C oracle`:
+/root/reference, or $HDDM_REF_TREE, or --ref) after `make -C oracle`:
 
     python tests/golden/make_golden.py
 
@@ -71,7 +71,7 @@ def run_ref(variant, plt, nagents, x):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("HDDM_REF_TREE", "/root/reference"))
     a = ap.parse_args()
     tdir = os.path.join(a.ref, "LinearBasis", "tests", "InterpolateArray")
     plt_src = os.path.join(tdir, "surplus.plt")

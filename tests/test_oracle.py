@@ -39,6 +39,45 @@ def test_oracle_matches_reference_gold_on_random_points():
     assert np.array_equal(g.index, r.index()) and np.array_equal(g.surplus, r.surplus())
 
 
+@pytest.mark.skipif(not O.ref_available("gold"), reason="reference not compiled here")
+@pytest.mark.parametrize("dim,nno,td,seed", [(59, 20000, 64, 3), (30, 8000, 32, 2), (16, 51137, 32, 1)])
+def test_oracle_bit_identical_to_reference_gold_on_generated_grids(tmp_path, dim, nno, td, seed):
+    """Generated grids (adaptive d=59 and d=30, regular d=16 level 5) written
+    as .plt and read back by the reference's own gold loader: the oracle's
+    reader gives the same arrays, and the oracle's kernel the reference gold
+    kernel's bits, on points of both distributions."""
+    import hddm_b200 as H
+    hg = H.HostGrid.regular(16, 5, 32, seed=seed) if dim == 16 else H.HostGrid.adaptive(dim, nno, td, seed=seed)
+    p = str(tmp_path / "grid.plt")
+    hg.write_plt(p)
+    g = O.Gold.read_plt(p, dim)
+    r = O.RefGrid(p, dim, "gold")
+    assert np.array_equal(g.index, r.index()) and np.array_equal(g.surplus, r.surplus())
+    X = H.gen_points(dim, 256, kind=2, seed=seed + 50)
+    assert np.array_equal(g.interpolate(X), r.interpolate(X))
+
+
+@pytest.mark.parametrize("dim,nno,td,seed", [(59, 30000, 16, 4), (30, 5000, 64, 203), (3, 40, 2, 9)])
+def test_oracle_generator_matches_product_generator(tmp_path, dim, nno, td, seed):
+    """The oracle's restatement of the seeded workload (used by the CPU
+    reference arm, which must not load the product library) gives the product
+    generator's grid and points array for array, and its .plt file reads back
+    to the same arrays."""
+    import hddm_b200 as H
+    og = O.Gold.adaptive(dim, nno, td, seed)
+    pi, ps = H.HostGrid.adaptive(dim, nno, td, seed=seed).arrays()
+    assert np.array_equal(og.index, pi) and np.array_equal(og.surplus, ps)
+    for kind, kr in ((0, 0.0), (1, 0.0), (2, 0.0), (0, 1e-6)):
+        assert np.array_equal(O.gen_points(dim, 301, kind, seed, kr), H.gen_points(dim, 301, kind, seed, kr)), kind
+    p = str(tmp_path / "g.plt")
+    og.write_plt(p)
+    back = O.Gold.read_plt(p, dim)
+    assert np.array_equal(back.index, pi) and np.array_equal(back.surplus, ps)
+    q = str(tmp_path / "h.plt")
+    H.HostGrid.adaptive(dim, nno, td, seed=seed).write_plt(q)
+    assert open(p, "rb").read() == open(q, "rb").read()
+
+
 def test_oracle_reader_rejects_bad_input(tmp_path):
     with pytest.raises(ValueError, match="mismatches config"):
         O.Gold.read_plt(PLT, 58)

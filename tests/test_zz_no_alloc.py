@@ -1,8 +1,8 @@
 """sgi_interpolate_noalloc: the forward pass for callers that must not allocate
-device memory (a solver whose device memory is all in its own arena, a first
-call made inside stream capture, a loop that cannot take cudaMalloc's implicit
-synchronization).  Its work counters live in a fixed array of the library's
-device image instead of a workspace allocated on first use.
+device memory (a solver whose device memory is all in its own arena, a loop
+that cannot take cudaMalloc's implicit synchronization).  Its work counters
+live in a fixed array of the library's device image instead of a workspace
+allocated on first use.
 
 Checked through the C ABI against sgi_interpolate, the entry point that
 allocates its workspace, on two calls in a row (the shared counter array keeps
@@ -64,6 +64,35 @@ def test_noalloc_matches_allocating_entry_point(cuda, counts):
             else:
                 assert np.array_equal(got, ref), (precision, call)
     assert O.rel_error(ref32, ref64)[0] <= 1e-7
+
+
+def test_noalloc_unchunked_matches_chunked_allocating_entry_point(cuda):
+    """sgi_interpolate walks large grids in node chunks, carrying the outputs
+    between launches; this entry launches every grid whole.  FP64 keeps gold's
+    order either way: the bits agree with a forced chunking of 1,000 nodes,
+    on two calls in a row.  FP32C stays within 1e-7 of FP64."""
+    import torch
+    hg = H.HostGrid.adaptive(59, 20000, 256, seed=45)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    X = H.gen_points(59, 6000, kind=2, seed=46)
+    x = torch.from_numpy(X).cuda()
+    prev = H.set_chunk_rows(1000)
+    try:
+        ref64 = H.interpolate(g, x, precision=H.FP64)
+        assert H.last_launch().kernels > 1        # node-chunked
+        ref64 = ref64.cpu().numpy()
+    finally:
+        H.set_chunk_rows(prev)
+    for precision in (H.FP64, H.FP32C):
+        for call in range(2):
+            out = torch.full((x.shape[0], 256), float("nan"), dtype=torch.float64, device="cuda")
+            assert _noalloc([g], x, [x.shape[0]], precision, out) == 0, H.lib.sgi_last_error().decode()
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            if precision == H.FP64:
+                assert np.array_equal(got, ref64), call
+            else:
+                assert O.rel_error(got, ref64)[0] <= 1e-7, call
 
 
 def test_noalloc_rejects_requests_beyond_its_scratch(cuda):
