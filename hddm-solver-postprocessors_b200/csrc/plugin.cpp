@@ -325,6 +325,38 @@ extern "C" void sgi_plugin_interpolate_multistate(Device* device, Data* data, co
 	getInterpolator()->interpolate(device, data, x, DofPerNode, value);
 }
 
+extern "C" void sgi_plugin_interpolate_batch(Device* device, Data* data_, int n, const int* istates,
+	const double* x, int DofPerNode, double* value)
+{
+	(void)device;
+	DataImpl* data = static_cast<DataImpl*>(data_);
+	check_dof(data, DofPerNode);
+	if (n < 0 || (n && (!istates || !x || !value))) die("Bad batch of %d points\n", n);
+	if (!n) return;
+	const int ns = data->nstates, dim = data->dim, TD = data->TotalDof;
+	// group the pairs by state (counting sort, stable), one call over the set
+	std::vector<long long> off(ns + 1, 0);
+	for (int k = 0; k < n; k++)
+	{
+		const int s = istates[k];
+		if (s < 0 || s >= ns || !data->loaded[s]) die("State %d is not loaded\n", s);
+		off[s + 1]++;
+	}
+	for (int s = 0; s < ns; s++) off[s + 1] += off[s];
+	std::vector<long long> pos(off.begin(), off.end() - 1);
+	std::vector<int> row(n);
+	std::vector<double> xb((size_t)n * dim), vb((size_t)n * TD);
+	for (int k = 0; k < n; k++)
+	{
+		const long long r = pos[istates[k]]++;
+		row[k] = (int)r;
+		memcpy(&xb[(size_t)r * dim], x + (size_t)k * dim, sizeof(double) * dim);
+	}
+	int rc = sgi_interpolate_host(ns, data->grids.data(), off.data(), xb.data(), vb.data(), SGI_FP64);
+	if (rc) die("%s\n", sgi_last_error());
+	for (int k = 0; k < n; k++) memcpy(value + (size_t)k * TD, &vb[(size_t)row[k] * TD], sizeof(double) * TD);
+}
+
 extern "C" void sgi_plugin_data_free(Data* data) { delete data; }
 
 extern "C" int sgi_plugin_device_index(const Device* device) { return device ? device->index : -1; }

@@ -1343,6 +1343,7 @@ __global__ void __launch_bounds__(LBLOCK) fwd_f64_list_kernel(const __grid_const
 // descriptor of the FP32C form), also the point's terms by the FP32C form's
 // classes: classes[3p] big (FP64 row), [3p + 1] fine (FP32 row), [3p + 2]
 // dropped, by the bound |w| * max|s_row| of the full-product weight.
+template <bool CLASSES>
 __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ FwdArgs a, long long* counts,
 	long long* classes)
 {
@@ -1361,7 +1362,7 @@ __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ Fw
 			traverse(G, xs, lane, [&](unsigned mask, int, double w, const uint4& r, float rm)
 			{
 				cnt += __popc(mask);
-				if (classes)
+				if (CLASSES)
 				{
 					const bool hit = (mask >> lane) & 1u;
 					const float bound = fabsf(__double2float_rn(w)) * rm;
@@ -1373,8 +1374,8 @@ __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ Fw
 			});
 		if (lane == 0)
 		{
-			if (counts) counts[p] = cnt;
-			if (classes)
+			if (!CLASSES) counts[p] = cnt;
+			else
 			{
 				classes[3 * p] = nbig;
 				classes[3 * p + 1] = nfine;
@@ -2510,11 +2511,12 @@ int count_terms(sgi_grid_t g, long long npts, const double* x, long long* counts
 	cudaStream_t s = (cudaStream_t)stream;
 	CUDA_TRY(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s));
 	const size_t smem = (size_t)WARPS * g->dim * sizeof(double);
-	if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	void (*kern)(FwdArgs, long long*, long long*) = classes ? count_kernel<true> : count_kernel<false>;
+	if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	int blocks = 0;
-	rc = occupancy_grid(count_kernel, smem, W->sms, &blocks);
+	rc = occupancy_grid(kern, smem, W->sms, &blocks);
 	if (rc) return rc;
-	count_kernel<<<blocks, BLOCK, smem, s>>>(a, counts, classes);
+	kern<<<blocks, BLOCK, smem, s>>>(a, counts, classes);
 	CUDA_TRY(cudaGetLastError());
 	return SGI_OK;
 }

@@ -148,6 +148,18 @@ void sgi_plugin_interpolate(SGI_PLUGIN_NAMESPACE::Device* device, SGI_PLUGIN_NAM
 void sgi_plugin_interpolate_multistate(SGI_PLUGIN_NAMESPACE::Device* device, SGI_PLUGIN_NAMESPACE::Data* data,
 	const double** x, int DofPerNode, double** value);
 void sgi_plugin_data_free(SGI_PLUGIN_NAMESPACE::Data* data);
+
+// Many (state, point) pairs in one call (no reference counterpart; the
+// reference takes one point of one state, or one point per state, per call:
+// include/interpolator.h:32-37).  Point k is x[k*dim .. k*dim + dim) of state
+// istates[k] (states may repeat, in any order); its values go to
+// value[k*DofPerNode ..].  The pairs are grouped by state and evaluated in
+// one batched forward over the states' grids (FP64 form: the same bits as n
+// single-state calls).  A solver's time step hands all its agents' points to
+// one call instead of one call per point.  Errors abort with the reference's
+// messages, as the Interpolator calls do.
+void sgi_plugin_interpolate_batch(SGI_PLUGIN_NAMESPACE::Device* device, SGI_PLUGIN_NAMESPACE::Data* data,
+	int n, const int* istates, const double* x, int DofPerNode, double* value);
 int sgi_plugin_device_index(const SGI_PLUGIN_NAMESPACE::Device* device);
 
 }

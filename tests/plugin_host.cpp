@@ -3,18 +3,27 @@
 // then virtual calls through the reference's class layouts declared in
 // include/sgi_plugin.h), without linking against it.
 //
-//   plugin_host <library> <grid.plt> <nstates> <x_0> ... <x_{dim-1}>
+//   plugin_host <library> <grid.plt[,grid2.plt,...]> <nstates> <x_0> ... <x_{dim-1}>
 //
-// Loads the grid file into every state of one Data object, then prints
+// Loads the grid files into the states of one Data object (state s takes
+// file s % nfiles), then prints
 //   single <v_0> ... <v_{TotalDof-1}>           interpolate(device, data, 0, x, ...)
 //   multi <s> <v_0> ... <v_{TotalDof-1}>        interpolate(device, data, xs, ...), per state
+//   batch <k> <s> <v_0> ...                     sgi_plugin_interpolate_batch over 2 * nstates
+//                                               (state, point) pairs: state (5k + 1) % nstates,
+//                                               point x_d + 0.01 k (mod 1) in every dimension d
+//   latency <n> <us per batch call> <us for n single calls>
 // with 17 significant digits.  hddm-solver.cfg must be in the working
 // directory (n_agents = the grid's dimension).  Exit status 2 when the
 // library or a symbol is missing or no GPU is supported.
 #include <dlfcn.h>
 
+#include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "sgi_plugin.h"
@@ -47,9 +56,20 @@ int main(int argc, char** argv)
 	std::vector<double> x;
 	for (int k = 4; k < argc; k++) x.push_back(atof(argv[k]));
 
+	auto batch = sym<void (*)(Device*, Data*, int, const int*, const double*, int, double*)>(
+		so, "sgi_plugin_interpolate_batch");
+	std::vector<std::string> files;
+	for (std::string rest = argv[2];;)
+	{
+		const size_t c = rest.find(',');
+		files.push_back(rest.substr(0, c));
+		if (c == std::string::npos) break;
+		rest = rest.substr(c + 1);
+	}
+
 	Interpolator* I = getInterp();
 	Data* data = getDataFn(nstates);
-	for (int s = 0; s < nstates; s++) data->load(argv[2], s);   // virtual
+	for (int s = 0; s < nstates; s++) data->load(files[s % files.size()].c_str(), s);   // virtual
 	Device* dev = acquire();
 	if (!dev) { fprintf(stderr, "no device acquired\n"); return 2; }
 
@@ -75,6 +95,36 @@ int main(int argc, char** argv)
 		for (int o = 0; o < TD; o++) printf(" %.17g", vals[s][o]);
 		printf("\n");
 	}
+	// many (state, point) pairs in one call
+	const int dim = (int)x.size(), n = 2 * nstates;
+	std::vector<int> st(n);
+	std::vector<double> xb((size_t)n * dim), vb((size_t)n * TD, 0.0);
+	for (int k = 0; k < n; k++)
+	{
+		st[k] = (5 * k + 1) % nstates;
+		for (int d = 0; d < dim; d++) xb[(size_t)k * dim + d] = std::fmod(x[d] + 0.01 * k, 1.0);
+	}
+	batch(dev, data, n, st.data(), xb.data(), TD, vb.data());
+	for (int k = 0; k < n; k++)
+	{
+		printf("batch %d %d", k, st[k]);
+		for (int o = 0; o < TD; o++) printf(" %.17g", vb[(size_t)k * TD + o]);
+		printf("\n");
+	}
+	// latency: one batch call against n single-state calls (best of 5)
+	using clk = std::chrono::steady_clock;
+	double tb = 1e30, ts = 1e30;
+	for (int rep = 0; rep < 5; rep++)
+	{
+		auto t0 = clk::now();
+		batch(dev, data, n, st.data(), xb.data(), TD, vb.data());
+		auto t1 = clk::now();
+		for (int k = 0; k < n; k++) I->interpolate(dev, data, st[k], &xb[(size_t)k * dim], TD, &vb[(size_t)k * TD]);
+		auto t2 = clk::now();
+		tb = std::min(tb, std::chrono::duration<double, std::micro>(t1 - t0).count());
+		ts = std::min(ts, std::chrono::duration<double, std::micro>(t2 - t1).count());
+	}
+	printf("latency %d %.1f %.1f\n", n, tb, ts);
 	release(dev);
 	data->clear();
 	delete data;

@@ -525,3 +525,25 @@ def test_small_batch_two_phase_exact(cuda, case):
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), ref)
     del plan
+
+
+def test_term_classes_partition_the_active_pairs(cuda):
+    """sgi_term_classes: big + fine + dropped = the active count per point; a
+    higher surplus cutoff only moves fine terms to dropped; an FP64-only grid
+    is refused."""
+    import torch
+    hg = H.HostGrid.adaptive(59, 20000, 64, seed=8)
+    g = H.Grid(hg, flags=H.BUILD_FP32)
+    x = torch.from_numpy(H.gen_points(59, 700, kind=2, seed=9)).cuda()
+    cnt = H.active_count(g, x).cpu().numpy()
+    c0 = H.term_classes(g, x).cpu().numpy()
+    assert np.array_equal(c0.sum(axis=1), cnt)
+    assert c0[:, 0].sum() > 0 and c0[:, 1].sum() > 0 and c0[:, 2].sum() > 0
+    smax = g.set_surplus_cutoff(0.0) * 2.0 ** 46
+    g.set_surplus_cutoff(smax * 2.0 ** -30)
+    c1 = H.term_classes(g, x).cpu().numpy()
+    g.set_surplus_cutoff(0.0)
+    assert np.array_equal(c1[:, 0], c0[:, 0]) and np.array_equal(c1.sum(axis=1), cnt)
+    assert (c1[:, 2] >= c0[:, 2]).all() and c1[:, 2].sum() > c0[:, 2].sum()
+    with pytest.raises(H.SgiError):
+        H.term_classes(H.Grid(hg), x)
