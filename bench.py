@@ -574,13 +574,44 @@ def run_multistate(args):
                                                           "large, avx2 (daint)": 4.234e-3}}))
 
 
+def run_load(args):
+    """Grid load time of the benchmark grid (d=59, 1M nodes, TotalDof 256)
+    from its .plt file: parse + layout build + upload, against a load through
+    the layout cache (the file's cache written by a first load)."""
+    import torch
+    import hddm_b200 as H
+    torch.cuda.init()
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "grid.plt")
+        H.HostGrid.adaptive(DIM, NNO, TD, seed=GRID_SEED).write_plt(p)
+        t = time.perf_counter()
+        hg = H.HostGrid.read_plt(p, DIM)
+        t_read = time.perf_counter() - t
+        g = H.Grid(hg, flags=H.BUILD_FP32)
+        t_build = time.perf_counter() - t
+        del g, hg
+        t = time.perf_counter()
+        g = H.Grid.load(p, DIM, flags=H.BUILD_FP32)
+        t_first = time.perf_counter() - t
+        del g
+        t = time.perf_counter()
+        g = H.Grid.load(p, DIM, flags=H.BUILD_FP32)
+        t_cached = time.perf_counter() - t
+        hit = g.cache_hit
+        sizes = {"plt_bytes": os.path.getsize(p), "cache_bytes": os.path.getsize(p + ".sgi-layout")}
+    print(json.dumps({"workload": "grid load: d=59, 1M nodes, TotalDof 256, FP64 + FP32C forms",
+                      "read_plt_s": t_read, "read_build_upload_s": t_build,
+                      "first_load_with_cache_write_s": t_first, "cached_load_s": t_cached, "cache_hit": hit,
+                      **sizes}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate"],
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c3", "multistate", "load"],
                     help="c4 (default) is the benchmark line; the others print their own measurements")
     ap.add_argument("--cpu-sample", type=int, default=16384,
                     help="points of the CPU baseline's timed sample (default: 16,384)")
@@ -607,6 +638,8 @@ def main():
         run_c3(args)
     elif args.workload == "multistate":
         run_multistate(args)
+    elif args.workload == "load":
+        run_load(args)
     else:
         run_gpu(args)
 

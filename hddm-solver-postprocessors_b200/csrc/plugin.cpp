@@ -136,25 +136,51 @@ public :
 		const Parameters& params = Interpolator::getInstance()->getParameters();
 		if (istate < 0 || istate >= nstates) die("State %d index out of range 0 .. %d\n", istate, nstates - 1);
 		if (loaded[istate]) die("State %d data is already loaded\n", istate);
-		sgi_host_grid_t hg = nullptr;
-		int rc = sgi_host_grid_read_plt(filename, params.nagents, &hg);
-		if (rc) die("%s\n", sgi_last_error());
-		int d = 0, nno = 0, td = 0;
-		sgi_host_grid_view(hg, &d, &nno, &td, nullptr, nullptr);
 		bool first = true;
 		for (int s = 0; s < nstates; s++) if (loaded[s]) first = false;
-		if (first) { dim = d; TotalDof = td; }
-		else
-		{
-			if (d != dim) { sgi_host_grid_free(hg); die("File \"%s\" # of dimensions (%d) mismatches another state (%d)\n", filename, d, dim); }
-			if (td != TotalDof) { sgi_host_grid_free(hg); die("File \"%s\" TotalDof (%d) mismatches another state (%d)\n", filename, td, TotalDof); }
-		}
 		int dev = 0;
 		cudaGetDevice(&dev);
 		sgi_grid_t g = nullptr;
-		rc = sgi_grid_create(hg, dev, 0u, &g);
-		sgi_host_grid_free(hg);
-		if (rc) die("%s\n", sgi_last_error());
+		int d = 0, td = 0;
+		// SGI_LAYOUT_CACHE: unset or "0" reads the file as the reference does;
+		// "1" keeps the built device layout in "<file>.sgi-layout"; any other
+		// value is a directory for those caches
+		const char* cache = getenv("SGI_LAYOUT_CACHE");
+		if (cache && *cache && strcmp(cache, "0"))
+		{
+			std::string cpath;
+			if (strcmp(cache, "1"))
+			{
+				const char* base = strrchr(filename, '/');
+				cpath = std::string(cache) + "/" + (base ? base + 1 : filename) + ".sgi-layout";
+			}
+			int rc = sgi_grid_load(filename, params.nagents, dev, 0u, cpath.empty() ? nullptr : cpath.c_str(), &g, nullptr);
+			if (rc) die("%s\n", sgi_last_error());
+			sgi_grid_info info;
+			sgi_grid_info_get(g, &info);
+			d = info.dim; td = info.TotalDof;
+		}
+		else
+		{
+			sgi_host_grid_t hg = nullptr;
+			int rc = sgi_host_grid_read_plt(filename, params.nagents, &hg);
+			if (rc) die("%s\n", sgi_last_error());
+			int nno = 0;
+			sgi_host_grid_view(hg, &d, &nno, &td, nullptr, nullptr);
+			if (!first && (d != dim || td != TotalDof)) sgi_host_grid_free(hg);
+			else
+			{
+				rc = sgi_grid_create(hg, dev, 0u, &g);
+				sgi_host_grid_free(hg);
+				if (rc) die("%s\n", sgi_last_error());
+			}
+		}
+		if (first) { dim = d; TotalDof = td; }
+		else
+		{
+			if (d != dim) { if (g) sgi_grid_destroy(g); die("File \"%s\" # of dimensions (%d) mismatches another state (%d)\n", filename, d, dim); }
+			if (td != TotalDof) { if (g) sgi_grid_destroy(g); die("File \"%s\" TotalDof (%d) mismatches another state (%d)\n", filename, td, TotalDof); }
+		}
 		grids[istate] = g;
 		loaded[istate] = true;
 	}

@@ -34,6 +34,8 @@
 // (fine) and dropped ones (negligible).
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
@@ -42,6 +44,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -1889,29 +1892,125 @@ extern "C" int sgi_device_count(void)
 }
 
 namespace {
-int chain_at(const sgi_grid* g, int c0, uint32_t* out);
-} // namespace
 
-extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, sgi_grid_t* out)
+template <class G>
+int chain_at(const G* g, int c0, uint32_t* out);
+
+// Everything sgi_grid_create uploads and keeps on the host, built from the
+// host grid: the device layout (records, components, containment tree,
+// descent groups, chain table), the surplus forms and the host copies the
+// launches need.  The layout cache stores it as it is.
+struct GridImage
 {
-	clear_error();
-	if (!hg || !out) return fail(SGI_E_INVALID, "null argument");
-	*out = nullptr;
-	const HostGrid& g = hg->g;
+	unsigned flags = 0;
+	int dim = 0, nno = 0, TD = 0, ld = 0, nlch = 0;
+	float skip_floor = 0.f;
+	std::vector<uint32_t> rec, comps, coarse_index, aux, ctab, grp_a, grp_b, ninfo;
+	std::vector<int> parent;
+	std::vector<double> s64, s64c;
+	std::vector<float> s32, rowmax;
+	std::vector<int> parent_h;
+	std::vector<uint32_t> skip_h, depth_h, gfirst_h, gcount_h, gcmin_h, gpmax_h;
+	sgi_grid_info info{};
+};
+
+int build_image(const HostGrid& g, unsigned flags, GridImage& im)
+{
 	if (g.nno > 0x7fffffff - 64) return fail(SGI_E_RANGE, "too many nodes");
-	int ndev = sgi_device_count();
-	if (ndev == 0) return fail(SGI_E_NODEVICE, "no CUDA device");
-	if (device < 0 || device >= ndev) return fail(SGI_E_INVALID, "device %d out of range (%d devices)", device, ndev);
 	DeviceLayout L;
 	int rc = build_layout(g, L);
 	if (rc) return rc;
-	DeviceGuard guard(device);
-	sgi_grid* d = new sgi_grid;
-	d->device = device; d->dim = g.dim; d->nno = g.nno; d->TD = g.TotalDof;
+	im.flags = flags;
+	im.dim = g.dim; im.nno = g.nno; im.TD = g.TotalDof;
 	// row stride: 32 for TotalDof <= 32 (a lane per output), else a multiple
 	// of 64 (a lane per output pair per 64 columns)
-	d->ld = g.TotalDof <= 32 ? 32 : (g.TotalDof + 63) / 64 * 64;
+	im.ld = g.TotalDof <= 32 ? 32 : (g.TotalDof + 63) / 64 * 64;
 	const size_t nrow = (size_t)std::max(g.nno, 1);
+	im.rec = L.rec; im.comps = L.comps; im.coarse_index = L.lo_index; im.parent = L.parent; im.aux = L.aux;
+	im.parent_h = L.parent;
+	im.skip_h.resize(g.nno);
+	im.depth_h.resize(g.nno);
+	for (int n = 0; n < g.nno; n++) { im.skip_h[n] = L.rec[4 * (size_t)n]; im.depth_h[n] = L.aux[2 * (size_t)n + 1]; }
+	if (g.nno > 0)
+	{
+		im.nlch = (g.nno + LCS - 1) / LCS;
+		im.ctab.assign((size_t)im.nlch * 32, 0u);
+		for (int k = 0; k < im.nlch; k++)
+			im.ctab[(size_t)k * 32] = (uint32_t)chain_at(&im, k * LCS, &im.ctab[(size_t)k * 32 + 1]);
+	}
+	if (!(flags & SGI_BUILD_NO_FP64))
+	{
+		im.s64.assign(nrow * im.ld, 0.0);
+		for (int n = 0; n < g.nno; n++)
+			memcpy(&im.s64[(size_t)n * im.ld], &g.surplus[(size_t)n * g.TotalDof], sizeof(double) * g.TotalDof);
+	}
+	if (flags & (SGI_BUILD_FP32 | SGI_BUILD_NO_FP64))
+	{
+		im.s32.assign(nrow * im.ld, 0.f);
+		im.s64c.assign((size_t)std::max(L.ncoarse, 1) * im.ld, 0.0);
+		for (int n = 0; n < g.nno; n++)
+			for (int o = 0; o < g.TotalDof; o++)
+			{
+				const double v = g.surplus[(size_t)n * g.TotalDof + o];
+				im.s32[(size_t)n * im.ld + o] = (float)v;
+				if (L.lo_index[n] != ~0u) im.s64c[(size_t)L.lo_index[n] * im.ld + o] = v;
+			}
+		// row maxima for the FP32C form's negligible-term test: a fine term is
+		// dropped when |w| * max|s_row| < 2^-46 * max|s| (at most ~2,000
+		// dropped terms per point: below 1e-10 of the largest surplus)
+		im.rowmax.assign(nrow, 0.f);
+		double smax = 0.0;
+		for (int n = 0; n < g.nno; n++)
+		{
+			double m = 0.0;
+			for (int o = 0; o < g.TotalDof; o++) m = std::max(m, fabs(g.surplus[(size_t)n * g.TotalDof + o]));
+			im.rowmax[n] = (float)(m * (1.0 + 0x1.0p-20));   // rounded up
+			smax = std::max(smax, m);
+		}
+		im.skip_floor = (float)(ldexp(smax, -46));
+		// descent layout: groups, and per node (plus the roots' virtual
+		// parent at index nno) {first group, group count, rowmax, FP64 copy row}
+		DescentLayout D;
+		rc = build_descent(g, L, D);
+		if (rc) return rc;
+		const size_t ng = D.cmin.size();
+		im.ninfo.resize((size_t)4 * (g.nno + 1));
+		for (int n = 0; n <= g.nno; n++)
+		{
+			im.ninfo[4 * (size_t)n + 0] = D.first[n];
+			im.ninfo[4 * (size_t)n + 1] = D.count[n];
+			im.ninfo[4 * (size_t)n + 2] = n < g.nno ? float_bits(im.rowmax[n]) : 0u;
+			im.ninfo[4 * (size_t)n + 3] = n < g.nno ? L.lo_index[n] : DESC_NONE;
+		}
+		im.grp_a = std::move(D.a);
+		im.grp_b = std::move(D.b);
+		im.gfirst_h = D.first;
+		im.gcount_h = D.count;
+		im.gcmin_h = D.cmin;
+		im.gpmax_h.resize(ng);
+		for (int n = 0; n <= g.nno; n++)
+		{
+			uint32_t m = 0;
+			for (uint32_t q = D.first[n]; q < D.first[n] + D.count[n]; q++) { m = std::max(m, D.cmax[q]); im.gpmax_h[q] = m; }
+		}
+	}
+	sgi_grid_info& I = im.info;
+	I.dim = g.dim; I.nno = g.nno; I.TotalDof = g.TotalDof; I.ld = im.ld;
+	I.max_comps = L.max_comps; I.tree_depth = L.tree_depth; I.tree_roots = L.tree_roots;
+	I.multi_delta = L.multi_delta; I.ncoarse = L.ncoarse; I.comps = (long long)L.comps.size() / 2;
+	I.device_bytes = 0; I.coarse_threshold = L.coarse_threshold;
+	return SGI_OK;
+}
+
+// Uploads an image to `device` (moving its host copies into the grid).
+int upload_image(GridImage& im, int device, sgi_grid_t* out)
+{
+	int ndev = sgi_device_count();
+	if (ndev == 0) return fail(SGI_E_NODEVICE, "no CUDA device");
+	if (device < 0 || device >= ndev) return fail(SGI_E_INVALID, "device %d out of range (%d devices)", device, ndev);
+	DeviceGuard guard(device);
+	sgi_grid* d = new sgi_grid;
+	d->device = device; d->dim = im.dim; d->nno = im.nno; d->TD = im.TD; d->ld = im.ld;
 	long long bytes = 0;
 	auto upload = [&](void** dst, const void* src, size_t n) -> int
 	{
@@ -1925,93 +2024,285 @@ extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, s
 		}
 		return SGI_OK;
 	};
-	rc = upload((void**)&d->rec, L.rec.data(), L.rec.size() * 4);
-	if (!rc) rc = upload((void**)&d->comps, L.comps.data(), L.comps.size() * 4);
-	if (!rc) rc = upload((void**)&d->coarse_index, L.lo_index.data(), L.lo_index.size() * 4);
-	if (!rc) rc = upload((void**)&d->parent, L.parent.data(), L.parent.size() * 4);
-	if (!rc) rc = upload((void**)&d->aux, L.aux.data(), L.aux.size() * 4);
-	d->parent_h = L.parent;
-	d->skip_h.resize(g.nno);
-	d->depth_h.resize(g.nno);
-	for (int n = 0; n < g.nno; n++) { d->skip_h[n] = L.rec[4 * (size_t)n]; d->depth_h[n] = L.aux[2 * (size_t)n + 1]; }
-	if (!rc && g.nno > 0)
+	int rc = upload((void**)&d->rec, im.rec.data(), im.rec.size() * 4);
+	if (!rc) rc = upload((void**)&d->comps, im.comps.data(), im.comps.size() * 4);
+	if (!rc) rc = upload((void**)&d->coarse_index, im.coarse_index.data(), im.coarse_index.size() * 4);
+	if (!rc) rc = upload((void**)&d->parent, im.parent.data(), im.parent.size() * 4);
+	if (!rc) rc = upload((void**)&d->aux, im.aux.data(), im.aux.size() * 4);
+	if (!rc && im.nno > 0) rc = upload((void**)&d->ctab, im.ctab.data(), im.ctab.size() * 4);
+	if (!rc && !im.s64.empty()) rc = upload((void**)&d->s64, im.s64.data(), im.s64.size() * 8);
+	if (!rc && !im.s32.empty())
 	{
-		d->nlch = (g.nno + LCS - 1) / LCS;
-		std::vector<uint32_t> t((size_t)d->nlch * 32, 0u);
-		for (int k = 0; k < d->nlch; k++) t[(size_t)k * 32] = (uint32_t)chain_at(d, k * LCS, &t[(size_t)k * 32 + 1]);
-		rc = upload((void**)&d->ctab, t.data(), t.size() * 4);
-	}
-	if (!rc && !(flags & SGI_BUILD_NO_FP64))
-	{
-		std::vector<double> s(nrow * d->ld, 0.0);
-		for (int n = 0; n < g.nno; n++)
-			memcpy(&s[(size_t)n * d->ld], &g.surplus[(size_t)n * g.TotalDof], sizeof(double) * g.TotalDof);
-		rc = upload((void**)&d->s64, s.data(), s.size() * 8);
-	}
-	if (!rc && (flags & (SGI_BUILD_FP32 | SGI_BUILD_NO_FP64)))
-	{
-		std::vector<float> hi(nrow * d->ld, 0.f);
-		std::vector<double> coarse((size_t)std::max(L.ncoarse, 1) * d->ld, 0.0);
-		for (int n = 0; n < g.nno; n++)
-			for (int o = 0; o < g.TotalDof; o++)
-			{
-				const double v = g.surplus[(size_t)n * g.TotalDof + o];
-				hi[(size_t)n * d->ld + o] = (float)v;
-				if (L.lo_index[n] != ~0u) coarse[(size_t)L.lo_index[n] * d->ld + o] = v;
-			}
-		rc = upload((void**)&d->s32, hi.data(), hi.size() * 4);
-		if (!rc) rc = upload((void**)&d->s64c, coarse.data(), coarse.size() * 8);
-		// row maxima for the FP32C form's negligible-term test: a fine term is
-		// dropped when |w| * max|s_row| < 2^-46 * max|s| (at most ~2,000
-		// dropped terms per point: below 1e-10 of the largest surplus)
-		std::vector<float> rmax(nrow, 0.f);
-		double smax = 0.0;
-		for (int n = 0; n < g.nno; n++)
-		{
-			double m = 0.0;
-			for (int o = 0; o < g.TotalDof; o++) m = std::max(m, fabs(g.surplus[(size_t)n * g.TotalDof + o]));
-			rmax[n] = (float)(m * (1.0 + 0x1.0p-20));   // rounded up
-			smax = std::max(smax, m);
-		}
-		if (!rc) rc = upload((void**)&d->rowmax, rmax.data(), rmax.size() * 4);
-		d->skip_floor = d->skip_below = (float)(ldexp(smax, -46));
-		// descent layout: groups, and per node (plus the roots' virtual
-		// parent at index nno) {first group, group count, rowmax, FP64 copy row}
-		DescentLayout D;
-		if (!rc) rc = build_descent(g, L, D);
-		if (!rc)
-		{
-			const size_t ng = D.cmin.size();
-			std::vector<uint32_t> ni((size_t)4 * (g.nno + 1));
-			for (int n = 0; n <= g.nno; n++)
-			{
-				ni[4 * (size_t)n + 0] = D.first[n];
-				ni[4 * (size_t)n + 1] = D.count[n];
-				ni[4 * (size_t)n + 2] = n < g.nno ? float_bits(rmax[n]) : 0u;
-				ni[4 * (size_t)n + 3] = n < g.nno ? L.lo_index[n] : DESC_NONE;
-			}
-			rc = upload((void**)&d->grp_a, D.a.data(), D.a.size() * 4);
-			if (!rc) rc = upload((void**)&d->grp_b, D.b.data(), D.b.size() * 4);
-			if (!rc) rc = upload((void**)&d->ninfo, ni.data(), ni.size() * 4);
-			d->gfirst_h = D.first;
-			d->gcount_h = D.count;
-			d->gcmin_h = D.cmin;
-			d->gpmax_h.resize(ng);
-			for (int n = 0; n <= g.nno; n++)
-			{
-				uint32_t m = 0;
-				for (uint32_t q = D.first[n]; q < D.first[n] + D.count[n]; q++) { m = std::max(m, D.cmax[q]); d->gpmax_h[q] = m; }
-			}
-		}
+		rc = upload((void**)&d->s32, im.s32.data(), im.s32.size() * 4);
+		if (!rc) rc = upload((void**)&d->s64c, im.s64c.data(), im.s64c.size() * 8);
+		if (!rc) rc = upload((void**)&d->rowmax, im.rowmax.data(), im.rowmax.size() * 4);
+		if (!rc) rc = upload((void**)&d->grp_a, im.grp_a.data(), im.grp_a.size() * 4);
+		if (!rc) rc = upload((void**)&d->grp_b, im.grp_b.data(), im.grp_b.size() * 4);
+		if (!rc) rc = upload((void**)&d->ninfo, im.ninfo.data(), im.ninfo.size() * 4);
 	}
 	if (rc) { free_grid(d); return rc; }
-	sgi_grid_info& I = d->info;
-	I.dim = g.dim; I.nno = g.nno; I.TotalDof = g.TotalDof; I.ld = d->ld;
-	I.max_comps = L.max_comps; I.tree_depth = L.tree_depth; I.tree_roots = L.tree_roots;
-	I.multi_delta = L.multi_delta; I.ncoarse = L.ncoarse; I.comps = (long long)L.comps.size() / 2;
-	I.device_bytes = bytes; I.coarse_threshold = L.coarse_threshold;
+	d->nlch = im.nlch;
+	d->skip_floor = d->skip_below = im.skip_floor;
+	d->parent_h = std::move(im.parent_h);
+	d->skip_h = std::move(im.skip_h);
+	d->depth_h = std::move(im.depth_h);
+	d->gfirst_h = std::move(im.gfirst_h);
+	d->gcount_h = std::move(im.gcount_h);
+	d->gcmin_h = std::move(im.gcmin_h);
+	d->gpmax_h = std::move(im.gpmax_h);
+	d->info = im.info;
+	d->info.device_bytes = bytes;
 	*out = d;
 	return SGI_OK;
+}
+
+// ------------------------------------------------------------ layout cache
+//
+// File: magic, format version, build flags, the .plt's size and modification
+// time (ns), then the image's scalars and arrays (element count, then the
+// raw elements, in a fixed order), then a 64-bit sum of every 8-byte word
+// written before it.  Native byte order: a cache is read back on the machine
+// (or an identical one) that wrote it.
+constexpr char CACHE_MAGIC[8] = { 'S', 'G', 'I', 'L', 'A', 'Y', 'O', 'T' };
+constexpr uint32_t CACHE_VERSION = 1;
+
+struct CacheKey
+{
+	int64_t size = 0, mtime_ns = 0;
+};
+
+int plt_key(const char* path, CacheKey* k)
+{
+	struct stat st;
+	if (stat(path, &st)) return fail(SGI_E_FORMAT, "Error opening file: %s", path);
+	k->size = (int64_t)st.st_size;
+	k->mtime_ns = (int64_t)st.st_mtim.tv_sec * 1000000000ll + st.st_mtim.tv_nsec;
+	return SGI_OK;
+}
+
+std::string cache_file(const char* path, const char* cache_path)
+{
+	return cache_path ? std::string(cache_path) : std::string(path) + ".sgi-layout";
+}
+
+struct CacheWriter
+{
+	FILE* f;
+	uint64_t sum = 0;
+	bool ok = true;
+	std::vector<unsigned char> pend;   // bytes not yet summed (partial word)
+	void raw(const void* p, size_t n)
+	{
+		if (!n) return;
+		if (fwrite(p, 1, n, f) != n) ok = false;
+		const unsigned char* c = (const unsigned char*)p;
+		size_t i = 0;
+		if (!pend.empty())
+		{
+			while (i < n && pend.size() < 8) pend.push_back(c[i++]);
+			if (pend.size() < 8) return;
+			uint64_t w; memcpy(&w, pend.data(), 8); sum += w; pend.clear();
+		}
+		for (; i + 8 <= n; i += 8) { uint64_t w; memcpy(&w, c + i, 8); sum += w; }
+		while (i < n) pend.push_back(c[i++]);
+	}
+	template <class T> void val(const T& v) { raw(&v, sizeof(T)); }
+	template <class T> void vec(const std::vector<T>& v) { val((uint64_t)v.size()); raw(v.data(), v.size() * sizeof(T)); }
+	// the sum with a trailing partial word zero-padded
+	uint64_t total()
+	{
+		uint64_t t = sum;
+		if (!pend.empty()) { unsigned char w8[8] = {0}; memcpy(w8, pend.data(), pend.size()); uint64_t w; memcpy(&w, w8, 8); t += w; }
+		return t;
+	}
+};
+
+struct CacheReader
+{
+	FILE* f;
+	uint64_t sum = 0;
+	bool ok = true;
+	std::vector<unsigned char> pend;
+	int64_t left;
+	void raw(void* p, size_t n)
+	{
+		if (!ok || !n) return;
+		if ((int64_t)n > left || fread(p, 1, n, f) != n) { ok = false; return; }
+		left -= (int64_t)n;
+		const unsigned char* c = (const unsigned char*)p;
+		size_t i = 0;
+		if (!pend.empty())
+		{
+			while (i < n && pend.size() < 8) pend.push_back(c[i++]);
+			if (pend.size() < 8) return;
+			uint64_t w; memcpy(&w, pend.data(), 8); sum += w; pend.clear();
+		}
+		for (; i + 8 <= n; i += 8) { uint64_t w; memcpy(&w, c + i, 8); sum += w; }
+		while (i < n) pend.push_back(c[i++]);
+	}
+	template <class T> void val(T& v) { raw(&v, sizeof(T)); }
+	template <class T> void vec(std::vector<T>& v)
+	{
+		uint64_t n = 0;
+		val(n);
+		if (!ok || n * sizeof(T) > (uint64_t)left) { ok = false; return; }
+		v.resize(n);
+		raw(v.data(), n * sizeof(T));
+	}
+	uint64_t total()
+	{
+		uint64_t t = sum;
+		if (!pend.empty()) { unsigned char w8[8] = {0}; memcpy(w8, pend.data(), pend.size()); uint64_t w; memcpy(&w, w8, 8); t += w; }
+		return t;
+	}
+};
+
+template <class IO, class Image>
+void cache_fields(IO& io, Image& im)
+{
+	io.val(im.dim); io.val(im.nno); io.val(im.TD); io.val(im.ld); io.val(im.nlch); io.val(im.skip_floor);
+	auto& I = im.info;
+	io.val(I.dim); io.val(I.nno); io.val(I.TotalDof); io.val(I.ld); io.val(I.max_comps); io.val(I.tree_depth);
+	io.val(I.tree_roots); io.val(I.multi_delta); io.val(I.ncoarse); io.val(I.comps); io.val(I.device_bytes);
+	io.val(I.coarse_threshold);
+	io.vec(im.rec); io.vec(im.comps); io.vec(im.coarse_index); io.vec(im.aux); io.vec(im.ctab);
+	io.vec(im.grp_a); io.vec(im.grp_b); io.vec(im.ninfo); io.vec(im.parent);
+	io.vec(im.s64); io.vec(im.s64c); io.vec(im.s32); io.vec(im.rowmax);
+	io.vec(im.parent_h); io.vec(im.skip_h); io.vec(im.depth_h);
+	io.vec(im.gfirst_h); io.vec(im.gcount_h); io.vec(im.gcmin_h); io.vec(im.gpmax_h);
+}
+
+// Writes the cache through a temporary file renamed into place, so that a
+// reader never sees a partial file.
+int write_cache(const GridImage& im, const CacheKey& key, const std::string& file)
+{
+	const std::string tmp = file + ".tmp" + std::to_string((long long)getpid());
+	FILE* f = fopen(tmp.c_str(), "wb");
+	if (!f) return fail(SGI_E_FORMAT, "cannot create %s", tmp.c_str());
+	setvbuf(f, nullptr, _IOFBF, 1 << 22);
+	CacheWriter w{ f };
+	w.raw(CACHE_MAGIC, 8);
+	w.val(CACHE_VERSION); w.val(im.flags); w.val(key.size); w.val(key.mtime_ns);
+	cache_fields(w, const_cast<GridImage&>(im));
+	const uint64_t sum = w.total();
+	w.pend.clear();
+	w.val(sum);
+	if (fclose(f)) w.ok = false;
+	if (!w.ok || rename(tmp.c_str(), file.c_str()))
+	{
+		unlink(tmp.c_str());
+		return fail(SGI_E_FORMAT, "cannot write the layout cache %s", file.c_str());
+	}
+	return SGI_OK;
+}
+
+// True (and the image filled) when `file` is a complete cache of this format
+// version for these build flags and this .plt key.
+bool read_cache(const std::string& file, unsigned flags, const CacheKey& key, GridImage& im)
+{
+	FILE* f = fopen(file.c_str(), "rb");
+	if (!f) return false;
+	setvbuf(f, nullptr, _IOFBF, 1 << 22);
+	struct stat st;
+	if (fstat(fileno(f), &st)) { fclose(f); return false; }
+	CacheReader r{ f };
+	r.left = (int64_t)st.st_size;
+	char magic[8];
+	uint32_t version = 0, fl = 0;
+	CacheKey k;
+	r.raw(magic, 8);
+	r.val(version); r.val(fl); r.val(k.size); r.val(k.mtime_ns);
+	bool ok = r.ok && !memcmp(magic, CACHE_MAGIC, 8) && version == CACHE_VERSION && fl == flags &&
+		k.size == key.size && k.mtime_ns == key.mtime_ns;
+	if (ok)
+	{
+		cache_fields(r, im);
+		const uint64_t sum = r.total();
+		r.pend.clear();
+		uint64_t stored = 0;
+		r.val(stored);
+		ok = r.ok && stored == sum && r.left == 0;
+	}
+	fclose(f);
+	if (ok) im.flags = flags;
+	return ok;
+}
+
+int image_from_plt(const char* path, int nagents, unsigned flags, GridImage& im)
+{
+	sgi_host_grid_t hg = nullptr;
+	int rc = sgi_host_grid_read_plt(path, nagents, &hg);
+	if (rc) return rc;
+	rc = build_image(hg->g, flags, im);
+	sgi_host_grid_free(hg);
+	return rc;
+}
+
+} // namespace
+
+extern "C" int sgi_grid_create(sgi_host_grid_t hg, int device, unsigned flags, sgi_grid_t* out)
+{
+	clear_error();
+	if (!hg || !out) return fail(SGI_E_INVALID, "null argument");
+	*out = nullptr;
+	int ndev = sgi_device_count();
+	if (ndev == 0) return fail(SGI_E_NODEVICE, "no CUDA device");
+	if (device < 0 || device >= ndev) return fail(SGI_E_INVALID, "device %d out of range (%d devices)", device, ndev);
+	GridImage im;
+	int rc = build_image(hg->g, flags, im);
+	if (rc) return rc;
+	return upload_image(im, device, out);
+}
+
+extern "C" int sgi_grid_load(const char* path, int nagents, int device, unsigned flags, const char* cache_path,
+	sgi_grid_t* out, int* hit)
+{
+	clear_error();
+	if (!path || !out) return fail(SGI_E_INVALID, "null argument");
+	*out = nullptr;
+	if (hit) *hit = 0;
+	int ndev = sgi_device_count();
+	if (ndev == 0) return fail(SGI_E_NODEVICE, "no CUDA device");
+	if (device < 0 || device >= ndev) return fail(SGI_E_INVALID, "device %d out of range (%d devices)", device, ndev);
+	CacheKey key;
+	int rc = plt_key(path, &key);
+	if (rc) return rc;
+	const std::string file = cache_file(path, cache_path);
+	GridImage im;
+	if (read_cache(file, flags, key, im) && im.dim == nagents)
+	{
+		if (hit) *hit = 1;
+		return upload_image(im, device, out);
+	}
+	im = GridImage{};
+	rc = image_from_plt(path, nagents, flags, im);
+	if (rc) return rc;
+	if (write_cache(im, key, file)) clear_error();   // a cache that cannot be written is not an error
+	return upload_image(im, device, out);
+}
+
+extern "C" int sgi_grid_cache_write(const char* path, int nagents, unsigned flags, const char* cache_path)
+{
+	clear_error();
+	if (!path) return fail(SGI_E_INVALID, "null argument");
+	CacheKey key;
+	int rc = plt_key(path, &key);
+	if (rc) return rc;
+	GridImage im;
+	rc = image_from_plt(path, nagents, flags, im);
+	if (rc) return rc;
+	return write_cache(im, key, cache_file(path, cache_path));
+}
+
+extern "C" int sgi_grid_cache_valid(const char* path, int nagents, unsigned flags, const char* cache_path)
+{
+	clear_error();
+	if (!path) return fail(SGI_E_INVALID, "null argument");
+	CacheKey key;
+	int rc = plt_key(path, &key);
+	if (rc) return rc;
+	GridImage im;
+	return read_cache(cache_file(path, cache_path), flags, key, im) && im.dim == nagents ? 1 : 0;
 }
 
 extern "C" int sgi_grid_info_get(sgi_grid_t g, sgi_grid_info* info)
@@ -2088,7 +2379,8 @@ int check_set(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets)
 // is the part of the ancestor path of the last live node before c0 that is
 // still open at c0; every ancestor of an open node is open, so the stored
 // depths run from 1 without gaps.
-int chain_at(const sgi_grid* g, int c0, uint32_t* out)
+template <class G>
+int chain_at(const G* g, int c0, uint32_t* out)
 {
 	if (c0 <= 0 || c0 >= g->nno) return 0;
 	int q = c0 - 1;

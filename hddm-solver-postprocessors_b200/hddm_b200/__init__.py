@@ -69,6 +69,9 @@ def _load():
         "sgi_grid_create": (I, [P, I, U, ctypes.POINTER(P)]),
         "sgi_grid_info_get": (I, [P, ctypes.POINTER(GridInfo)]),
         "sgi_grid_destroy": (None, [P]),
+        "sgi_grid_load": (I, [ctypes.c_char_p, I, I, U, ctypes.c_char_p, ctypes.POINTER(P), _c_int_p]),
+        "sgi_grid_cache_write": (I, [ctypes.c_char_p, I, U, ctypes.c_char_p]),
+        "sgi_grid_cache_valid": (I, [ctypes.c_char_p, I, U, ctypes.c_char_p]),
         "sgi_grid_set_surplus_cutoff": (I, [P, D, ctypes.POINTER(D)]),
         "sgi_interpolate": (I, [I, P, P, P, P, I, P]),
         "sgi_interpolate_host": (I, [I, P, P, P, P, I]),
@@ -216,6 +219,19 @@ class HostGrid:
         return a, b, first, count, npr.value
 
 
+def cache_write(path, nagents, flags=0, cache_path=None):
+    """Build the layout of a .plt grid on the host and write its cache (no GPU)."""
+    _check(lib.sgi_grid_cache_write(os.fsencode(path), nagents, flags,
+                                    os.fsencode(cache_path) if cache_path else None))
+
+
+def cache_valid(path, nagents, flags=0, cache_path=None):
+    rc = lib.sgi_grid_cache_valid(os.fsencode(path), nagents, flags, os.fsencode(cache_path) if cache_path else None)
+    if rc < 0:
+        _check(rc)
+    return rc == 1
+
+
 def gen_points(dim, npts, kind=0, seed=0, kink_reject=0.0, max_level=7):
     out = np.zeros((npts, dim), np.float64)
     _check(lib.sgi_gen_points(dim, npts, kind, seed, kink_reject, max_level, out.ctypes.data))
@@ -251,6 +267,21 @@ class Grid:
     @property
     def handle(self):
         return self._h
+
+    @classmethod
+    def load(cls, path, nagents, device=0, flags=0, cache_path=None):
+        """A .plt grid through the layout cache (see sgi_grid_load); the
+        grid's `cache_hit` tells whether the cache was used."""
+        h = ctypes.c_void_p()
+        hit = ctypes.c_int()
+        _check(lib.sgi_grid_load(os.fsencode(path), nagents, device, flags,
+                                 os.fsencode(cache_path) if cache_path else None, ctypes.byref(h), ctypes.byref(hit)))
+        g = cls.__new__(cls)
+        g._h = h
+        g.device = device
+        g.info = g.get_info()
+        g.cache_hit = bool(hit.value)
+        return g
 
     def get_info(self):
         info = GridInfo()

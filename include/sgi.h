@@ -153,6 +153,36 @@ int sgi_grid_create(sgi_host_grid_t g, int device, unsigned flags, sgi_grid_t* o
 int sgi_grid_info_get(sgi_grid_t g, sgi_grid_info* info);
 void sgi_grid_destroy(sgi_grid_t g);
 
+/* Load a .plt grid file onto `device` through a cache of its built device
+ * layout (the containment tree, descent groups, chain table and surplus
+ * forms that sgi_grid_create builds on the host from the file's arrays).
+ * cache_path NULL means "<path>.sgi-layout".  When the cache is complete,
+ * of this library's format version, built with the same flags and for the
+ * same .plt (its size and modification time, to the nanosecond), the layout
+ * is read from it and uploaded: the .plt is not parsed and nothing is
+ * rebuilt.  Otherwise the .plt is read (nagents checked against its header,
+ * as sgi_host_grid_read_plt does), the layout built and uploaded, and the
+ * cache written through a temporary file renamed into place (a cache that
+ * cannot be written is not an error).  *hit (may be NULL) is 1 when the
+ * cache was used.  The result is the grid sgi_grid_create makes from the
+ * same file, and computes the same bits.  The cache is a native-byte-order
+ * file for this library build; it holds the FP64 surplus rows too, so it is
+ * larger than a compressed .plt.  Replaces the parse and the per-load
+ * layout work of the reference's Data::load
+ * (LinearBasis/gold/src/Data.cpp:322-595, LinearBasis/x86/src/Data.cpp:598-951),
+ * which has no cache. */
+int sgi_grid_load(const char* path, int nagents, int device, unsigned flags, const char* cache_path,
+	sgi_grid_t* out, int* hit);
+
+/* The cache half of sgi_grid_load without a GPU: build the layout of `path`
+ * on the host and write its cache (cache_path NULL: "<path>.sgi-layout"). */
+int sgi_grid_cache_write(const char* path, int nagents, unsigned flags, const char* cache_path);
+
+/* 1 when the cache of `path` is valid for these flags and nagents (its key,
+ * version and checksum match), 0 when sgi_grid_load would rebuild it, or a
+ * negative SGI_E_* code (the .plt itself is missing). */
+int sgi_grid_cache_valid(const char* path, int nagents, unsigned flags, const char* cache_path);
+
 /* Surplus cutoff of the FP32C form.  The reference parses a surplusCutoff
  * parameter (LinearBasis/cpu/src/parameters.cpp:103-108,
  * LinearBasis/cuda/src/parameters.cpp:110-127) and no kernel reads it; here

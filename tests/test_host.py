@@ -343,3 +343,36 @@ def test_descent_stack_stays_within_capacity(kind):
     assert depth <= SCAP - 32
     for x in H.gen_points(dim, 8, kind=2, seed=3):
         assert _stack_peak(desc, x, depth) <= SCAP
+
+
+def test_layout_cache_file(tmp_path):
+    """The layout cache without a GPU: written deterministically, valid for
+    its own .plt, flags and nagents, invalid once the .plt changes (size or
+    modification time) or the file is damaged."""
+    import os
+    p = str(tmp_path / "g.plt")
+    H.HostGrid.adaptive(30, 3000, 40, seed=5).write_plt(p)
+    c1, c2 = str(tmp_path / "a.cache"), str(tmp_path / "b.cache")
+    assert not H.cache_valid(p, 30, H.BUILD_FP32, c1)
+    H.cache_write(p, 30, H.BUILD_FP32, c1)
+    H.cache_write(p, 30, H.BUILD_FP32, c2)
+    assert open(c1, "rb").read() == open(c2, "rb").read()
+    assert H.cache_valid(p, 30, H.BUILD_FP32, c1)
+    assert not H.cache_valid(p, 30, 0, c1)          # other build flags
+    assert not H.cache_valid(p, 29, H.BUILD_FP32, c1)
+    # the default name sits beside the .plt
+    H.cache_write(p, 30, 0)
+    assert os.path.exists(p + ".sgi-layout") and H.cache_valid(p, 30, 0)
+    # damage: one flipped byte in the middle, or a truncated file
+    b = bytearray(open(c1, "rb").read())
+    b[len(b) // 2] ^= 0x40
+    open(c2, "wb").write(bytes(b))
+    assert not H.cache_valid(p, 30, H.BUILD_FP32, c2)
+    open(c2, "wb").write(bytes(b[: len(b) - 100]))
+    assert not H.cache_valid(p, 30, H.BUILD_FP32, c2)
+    # a rewritten .plt (new modification time) makes the cache stale
+    st = os.stat(p)
+    os.utime(p, ns=(st.st_atime_ns, st.st_mtime_ns + 1000))
+    assert not H.cache_valid(p, 30, H.BUILD_FP32, c1)
+    with pytest.raises(H.SgiError):
+        H.cache_write(str(tmp_path / "missing.plt"), 30, 0)
