@@ -86,8 +86,9 @@ def make_workload(npts=NPTS, seed_offset=0):
 def alg_bytes(hg, info, npts, fp32c):
     """Algorithmic bytes of one forward call, each grid array counted once:
     coordinates and outputs (FP64) per point, the surplus rows (FP32 for FP32C,
-    FP64 for the FP64 form), for FP32C the FP64 copies of the coarse rows,
-    chains (2 B per node per non-constant dimension) and unique xps (4 B)."""
+    FP64 for the FP64 form), for FP32C also the FP64 copies of the coarse rows
+    and the FP16 rows, chains (2 B per node per non-constant dimension) and
+    unique xps (4 B)."""
     idx, _ = hg.arrays()
     i = idx[:, :DIM]
     j = idx[:, DIM:]
@@ -95,7 +96,7 @@ def alg_bytes(hg, info, npts, fp32c):
     dims = np.broadcast_to(np.arange(DIM), i.shape)[nz].astype(np.int64)
     keys = (dims << 32) | (i[nz].astype(np.int64) << 16) | j[nz].astype(np.int64)
     szxps = int(np.unique(keys).size) + 1
-    rows = info.nno * TD * 4 + info.ncoarse * TD * 8 if fp32c else info.nno * TD * 8
+    rows = info.nno * TD * 4 + info.ncoarse * TD * 8 + info.nno * TD * 2 if fp32c else info.nno * TD * 8
     return npts * DIM * 8 + npts * TD * 8 + rows + 2 * info.nno * info.max_comps + 4 * szxps, szxps
 
 
@@ -275,7 +276,7 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
     walk_ms = e0.elapsed_time(e1)
     pairs = float(counts.double().sum())
-    n_big, n_fine, n_drop = (float(v) for v in classes.cpu())
+    n_big, n_fine, n_half, n_drop = (float(v) for v in classes.cpu())
     o64_sub = o32_sub = None
     if world == 1 and npts == NPTS:
         sub = torch.from_numpy(check_subsample()).to(dev)
@@ -293,7 +294,7 @@ def run_gpu(args):
         pts_s = npts * world / (ms32 * 1e-3)
         pts64_s = npts * world / (ms64 * 1e-3)
         ach = b32 / (ms32 * 1e-3) / 1e9
-        gather_b = n_fine * info.ld * 4 + n_big * info.ld * 8
+        gather_b = n_fine * info.ld * 4 + n_half * info.ld * 2 + n_big * info.ld * 8
         warps = VARIANT_WARPS.get(plan32.variant % 3, 32)
         gpeak = GATHER_PEAK_TBS[64 if warps > 32 else 32]
         gach = gather_b / (ms32 * 1e-3) / 1e12
@@ -333,10 +334,12 @@ def run_gpu(args):
                                 "peak": gpeak, "frac": gach / gpeak, "peak_64_warps_per_sm": GATHER_PEAK_TBS[64],
                                 "frac_of_64_warp_peak": gach / GATHER_PEAK_TBS[64],
                                 "bytes_per_call": gather_b, "kernel_warps_per_sm": warps,
-                                "terms": {"big_fp64_rows": n_big, "fine_fp32_rows": n_fine, "dropped": n_drop},
-                                "note": "rows the FP32C kernel reads: fine terms x TotalDof x 4 B + big terms x "
-                                        "TotalDof x 8 B (dropped terms read none), over the step time; peak: random "
-                                        "1 KB row gathers from L2 at the kernel's warps per SM"},
+                                "terms": {"big_fp64_rows": n_big, "fine_fp32_rows": n_fine,
+                                          "fine_fp16_rows": n_half, "dropped": n_drop},
+                                "note": "rows the FP32C kernel reads: fine terms x TotalDof x 4 B (FP32 rows) or "
+                                        "x 2 B (FP16 rows) + big terms x TotalDof x 8 B (dropped terms read none), "
+                                        "over the step time; peak: random 1 KB row gathers from L2 at the kernel's "
+                                        "warps per SM"},
             "fma_work": {"active_pairs_per_call": pairs, "flops_per_call": flops,
                          "achieved_tflops": flops / (ms32 * 1e-3) / 1e12,
                          "fp32_peak_tflops": fp32_peak, "frac": flops / (ms32 * 1e-3) / 1e12 / fp32_peak,

@@ -74,9 +74,11 @@ struct GridDesc
 	const uint4* grp_a;          // descent child groups (FP32C): {L, R, d | kind << 16, parent's ij in d}
 	const uint2* grp_b;          //   {L's ij in d, R's}
 	const uint4* ninfo;          //   per node: {first group, group count, rowmax bits, FP64 copy row or NONE}
+	const uint4* s16;            // FP16 rows (FP32C), per 256 outputs in lane order; see build_image
 	int depth;                   // containment-tree depth (bounds the descent stack)
 	float skip_below;            // FP32C drops fine terms with |w| * rowmax below this
 	float big_below;             // FP32C: terms with |w| * rowmax from this up are big (FP64 rows)
+	float f16_below;             // FP32C: fine terms with |w| * rowmax below this read the FP16 rows (0: none)
 	long long pt_begin;
 	int nno;
 	int ld;
@@ -558,9 +560,10 @@ __host__ __device__ __forceinline__ int list_stride(int dim) { return FCAP + WPA
 // The other ("fine") terms, each below the threshold, are appended to a
 // per-warp list of {row, FP32 weight} entries and gathered in FP32 in groups
 // of Q rows; their FP32 partial sums are added to the outputs' FP64 running
-// sums every FLUSH terms.  Fine terms below 2^-46 of the largest surplus are
-// dropped before their row is read.  The running sums also carry the outputs
-// across node chunks.
+// sums every FLUSH terms.  Fine terms below 2^-42 of the largest surplus are
+// dropped before their row is read; in the descent form, fine terms below
+// 2^-32 of it read FP16 copies of their rows (see half_lo_scaled).  The
+// running sums also carry the outputs across node chunks.
 constexpr int FLUSH = 8;
 
 template <int V, int E, int Q, int MINB>
@@ -773,8 +776,30 @@ constexpr int SCAP = 96;
 
 // Shared memory per warp of the descent form, in doubles: the stack (SCAP
 // 16-byte entries), the fine-term list (whose first 32 doubles hold the chain
-// weights at a chunk start, before any term is listed) and the point.
-__host__ __device__ __forceinline__ int desc_stride(int dim) { return 2 * SCAP + FCAP + ((dim + 1) & ~1); }
+// weights at a chunk start, before any term is listed), the list of fine
+// terms read from FP16 rows, and the point.
+__host__ __device__ __forceinline__ int desc_stride(int dim) { return 2 * SCAP + 2 * FCAP + ((dim + 1) & ~1); }
+
+// FP16 rows: row n holds its surpluses times 2^k_n as IEEE half precision,
+// k_n = 14 - floor(log2(rowmax_n)), so that the row's largest magnitude lies
+// in [2^14, 2^15).  Within each block of 256 outputs, lane l's 16 bytes hold
+// outputs 128 v + 4 l + e (v = 0, 1; e = 0..3) in that order: the outputs the
+// lane owns in the two-by-four output layout, one 16-byte load per row.
+// Moving a half's bits up by 13 (sign up by 16) gives an FP32 of its value
+// times 2^-112, subnormal halves included; the term's weight is scaled by
+// 2^(112 - k_n) = 2^(98 + floor(log2(rowmax_n))) when it is listed.
+__device__ __forceinline__ float half_lo_scaled(uint32_t u)
+{
+	return __uint_as_float(((u << 16) & 0x80000000u) | ((u << 13) & 0x0fffe000u));
+}
+__device__ __forceinline__ float half_hi_scaled(uint32_t u)
+{
+	return __uint_as_float((u & 0x80000000u) | ((u >> 3) & 0x0fffe000u));
+}
+__device__ __forceinline__ float f16_weight(float wf, uint32_t rowmax_bits)
+{
+	return wf * __uint_as_float((((rowmax_bits >> 23) & 0xffu) + 98u) << 23);
+}
 static_assert(FCAP >= 32, "the chain weights (32 doubles) alias the fine-term list");
 
 __device__ __forceinline__ uint4 pack_seg(uint32_t b, uint32_t e, double w)
@@ -793,7 +818,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 	uint4* stk = reinterpret_cast<uint4*>(wbase);
 	uint2* fl = reinterpret_cast<uint2*>(wbase + 2 * SCAP);
 	double* wchain = wbase + 2 * SCAP;     // aliases fl: used before any term is listed
-	double* xs = wbase + 2 * SCAP + FCAP;
+	uint2* fl16 = reinterpret_cast<uint2*>(wbase + 2 * SCAP + FCAP);
+	double* xs = wbase + 2 * SCAP + 2 * FCAP;
+	// FP16 rows serve launches whose lanes own two blocks of four outputs of
+	// full 256-output passes (the layout of the rows)
+	constexpr bool F16 = V == 2 && E == 4 && FULLROW;
+	constexpr int Q16 = 2 * Q;   // FP16 rows per group: the registers of Q FP32 rows
 	const bool first = a.chunk_begin == 0;
 	for (;;)
 	{
@@ -848,13 +878,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 			const double* s64l = G.s64c + lcol;
 			const uint32_t ld = (uint32_t)G.ld;
 			const float skip_below = G.skip_below, big_below = G.big_below;
+			const float f16_below = F16 && G.s16 ? G.f16_below : 0.f;
+			const uint4* s16l = G.s16 + (a.o_begin >> 8) * 32 + lane;
+			const uint32_t ld16 = (uint32_t)G.ld >> 3;
 			const int room = SCAP - G.depth;        // steps of min(32, room - size) groups
 			float part[V][E];
 #pragma unroll
 			for (int v = 0; v < V; v++)
 #pragma unroll
 				for (int e = 0; e < E; e++) part[v][e] = 0.f;
-			int cnt = 0, since = 0;
+			int cnt = 0, cnt16 = 0, since = 0;
 			auto flush = [&]()
 			{
 #pragma unroll
@@ -896,6 +929,39 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 							for (int q = 0; q < Q; q++)
 								part[v][e] = __fmaf_rn(__uint_as_float(en[q].y), sv[q][v][e], part[v][e]);
 					since += Q;
+					if (since >= FLUSH) { flush(); since = 0; }
+				}
+			};
+			// FP16 list entries [h, hend), hend - h a multiple of Q16
+			auto groups16 = [&](int h, int hend)
+			{
+				for (; h < hend; h += Q16)
+				{
+					uint2 en[Q16];
+#pragma unroll
+					for (int q = 0; q < Q16; q += 2)
+					{
+						const uint4 t = *reinterpret_cast<const uint4*>(fl16 + h + q);
+						en[q] = make_uint2(t.x, t.y);
+						en[q + 1] = make_uint2(t.z, t.w);
+					}
+					uint4 hv[Q16];
+#pragma unroll
+					for (int q = 0; q < Q16; q++) hv[q] = __ldg(s16l + (size_t)en[q].x * ld16);
+#pragma unroll
+					for (int q = 0; q < Q16; q++)
+					{
+						const float w = __uint_as_float(en[q].y);
+						part[0][0] = __fmaf_rn(w, half_lo_scaled(hv[q].x), part[0][0]);
+						part[0][1] = __fmaf_rn(w, half_hi_scaled(hv[q].x), part[0][1]);
+						part[0][2] = __fmaf_rn(w, half_lo_scaled(hv[q].y), part[0][2]);
+						part[0][3] = __fmaf_rn(w, half_hi_scaled(hv[q].y), part[0][3]);
+						part[V - 1][0] = __fmaf_rn(w, half_lo_scaled(hv[q].z), part[V - 1][0]);
+						part[V - 1][1] = __fmaf_rn(w, half_hi_scaled(hv[q].z), part[V - 1][1]);
+						part[V - 1][2] = __fmaf_rn(w, half_lo_scaled(hv[q].w), part[V - 1][2]);
+						part[V - 1][3] = __fmaf_rn(w, half_hi_scaled(hv[q].w), part[V - 1][3]);
+					}
+					since += Q16;
 					if (since >= FLUSH) { flush(); since = 0; }
 				}
 			};
@@ -974,10 +1040,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 				const float bound = fabsf(wf) * __uint_as_float(ni.z);
 				const bool big = hit && ni.w != DESC_NONE && bound >= big_below;
 				const bool fine = hit && !big && bound >= skip_below;
+				const bool half = fine && bound < f16_below;
 				unsigned cm = __ballot_sync(FULL, big);
-				const unsigned fm = __ballot_sync(FULL, fine);
-				if (fine) fl[cnt + __popc(fm & ((1u << lane) - 1u))] = make_uint2(c, __float_as_uint(wf));
+				const unsigned fm = __ballot_sync(FULL, fine && !half);
+				const unsigned hm = __ballot_sync(FULL, half);
+				const unsigned below = (1u << lane) - 1u;
+				if (fine && !half) fl[cnt + __popc(fm & below)] = make_uint2(c, __float_as_uint(wf));
+				if (half) fl16[cnt16 + __popc(hm & below)] = make_uint2(c, __float_as_uint(f16_weight(wf, ni.z)));
 				cnt += __popc(fm);
+				cnt16 += __popc(hm);
 				while (cm)
 				{
 					const int k0 = __ffs(cm) - 1;
@@ -1020,6 +1091,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 					__syncwarp();
 					cnt = rem;
 				}
+				if (F16 && cnt16 >= 32)
+				{
+					__syncwarp();
+					const int wholeq = cnt16 - cnt16 % Q16;
+					groups16(0, wholeq);
+					const int rem = cnt16 - wholeq;
+					uint2 t = make_uint2(0u, 0u);
+					if (lane < rem) t = fl16[wholeq + lane];
+					__syncwarp();
+					if (lane < rem) fl16[lane] = t;
+					__syncwarp();
+					cnt16 = rem;
+				}
 			}
 			if (cnt)
 			{
@@ -1030,6 +1114,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 				if (lane >= cnt && lane < padded) fl[lane] = make_uint2(r0, 0u);
 				__syncwarp();
 				groups(0, padded);
+			}
+			if (F16 && cnt16)
+			{
+				const int padded = (cnt16 + Q16 - 1) / Q16 * Q16;
+				__syncwarp();
+				const uint32_t r0 = fl16[0].x;
+				if (lane >= cnt16 && lane < padded) fl16[lane] = make_uint2(r0, 0u);
+				__syncwarp();
+				groups16(0, padded);
 			}
 			flush();
 		}
@@ -1344,8 +1437,9 @@ __global__ void __launch_bounds__(LBLOCK) fwd_f64_list_kernel(const __grid_const
 
 // Active-node count per point (single grid).  With `classes` (a grid
 // descriptor of the FP32C form), also the point's terms by the FP32C form's
-// classes: classes[3p] big (FP64 row), [3p + 1] fine (FP32 row), [3p + 2]
-// dropped, by the bound |w| * max|s_row| of the full-product weight.
+// classes: classes[4p] big (FP64 row), [4p + 1] fine (FP32 row), [4p + 2]
+// fine (FP16 row), [4p + 3] dropped, by the bound |w| * max|s_row| of the
+// full-product weight.
 template <bool CLASSES>
 __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ FwdArgs a, long long* counts,
 	long long* classes)
@@ -1360,7 +1454,7 @@ __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ Fw
 		p = __shfl_sync(FULL, p, 0);
 		if (p >= a.npts) break;
 		const GridDesc& G = a.g[find_grid(a, p)];
-		long long cnt = 0, nbig = 0, nfine = 0;
+		long long cnt = 0, nbig = 0, nfine = 0, nhalf = 0;
 		if (load_point(a, p, xs, lane))
 			traverse(G, xs, lane, [&](unsigned mask, int, double w, const uint4& r, float rm)
 			{
@@ -1371,8 +1465,10 @@ __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ Fw
 					const float bound = fabsf(__double2float_rn(w)) * rm;
 					const bool big = hit && (r.z & NODE_COARSE) && bound >= G.big_below;
 					const bool fine = hit && !big && bound >= G.skip_below;
+					const bool half = fine && bound < G.f16_below;
 					nbig += __popc(__ballot_sync(FULL, big));
-					nfine += __popc(__ballot_sync(FULL, fine));
+					nfine += __popc(__ballot_sync(FULL, fine && !half));
+					nhalf += __popc(__ballot_sync(FULL, half));
 				}
 			});
 		if (lane == 0)
@@ -1380,9 +1476,10 @@ __global__ void __launch_bounds__(BLOCK) count_kernel(const __grid_constant__ Fw
 			if (!CLASSES) counts[p] = cnt;
 			else
 			{
-				classes[3 * p] = nbig;
-				classes[3 * p + 1] = nfine;
-				classes[3 * p + 2] = cnt - nbig - nfine;
+				classes[4 * p] = nbig;
+				classes[4 * p + 1] = nfine;
+				classes[4 * p + 2] = nhalf;
+				classes[4 * p + 3] = cnt - nbig - nfine - nhalf;
 			}
 		}
 		__syncwarp();
@@ -1805,7 +1902,9 @@ struct sgi_grid
 	uint2* comps = nullptr;
 	float* rowmax = nullptr;
 	float skip_below = 0.f;      // in use: the larger of skip_floor and the surplus cutoff
-	float skip_floor = 0.f;      // FP32C's own negligible-term bound, 2^-46 of max |surplus|
+	float skip_floor = 0.f;      // FP32C's own negligible-term bound, 2^-42 of max |surplus|
+	float f16_floor = 0.f;       // FP32C: fine terms below this bound read the FP16 rows (2^-32 of max |surplus|)
+	uint4* s16 = nullptr;        // FP16 rows (see the kernels' description), or null
 	uint2* aux = nullptr;
 	double* s64 = nullptr;
 	float* s32 = nullptr;
@@ -1855,6 +1954,7 @@ void free_grid(sgi_grid* g)
 	cudaFree(g->aux);
 	cudaFree(g->grp_a); cudaFree(g->grp_b); cudaFree(g->ninfo);
 	cudaFree(g->ctab);
+	cudaFree(g->s16);
 	cudaSetDevice(prev);
 	delete g;
 }
@@ -1872,6 +1972,8 @@ GridDesc desc_of(const sgi_grid* g, long long pt_begin, int precision = SGI_FP64
 	d.s64 = g->s64; d.s32 = g->s32; d.s64c = g->s64c;
 	d.coarse_index = g->coarse_index; d.parent = g->parent; d.pt_begin = pt_begin; d.nno = g->nno; d.ld = g->ld;
 	d.grp_a = g->grp_a; d.grp_b = g->grp_b; d.ninfo = g->ninfo; d.depth = g->info.tree_depth;
+	d.s16 = precision == SGI_FP32C ? g->s16 : nullptr;
+	d.f16_below = precision == SGI_FP32C && g->s16 ? g->f16_floor : 0.f;
 	return d;
 }
 
@@ -1904,8 +2006,9 @@ struct GridImage
 {
 	unsigned flags = 0;
 	int dim = 0, nno = 0, TD = 0, ld = 0, nlch = 0;
-	float skip_floor = 0.f;
+	float skip_floor = 0.f, f16_floor = 0.f;
 	std::vector<uint32_t> rec, comps, coarse_index, aux, ctab, grp_a, grp_b, ninfo;
+	std::vector<uint16_t> s16;
 	std::vector<int> parent;
 	std::vector<double> s64, s64c;
 	std::vector<float> s32, rowmax;
@@ -1913,6 +2016,25 @@ struct GridImage
 	std::vector<uint32_t> skip_h, depth_h, gfirst_h, gcount_h, gcmin_h, gpmax_h;
 	sgi_grid_info info{};
 };
+
+// IEEE binary16 bits of v, rounded to nearest (ties to even); |v| < 65504.
+uint16_t half_bits(double v)
+{
+	const uint16_t sign = std::signbit(v) ? 0x8000u : 0u;
+	const double a = fabs(v);
+	if (a == 0.0) return sign;
+	int ex = 0;
+	frexp(a, &ex);                                 // a in [2^(ex-1), 2^ex)
+	if (ex - 1 >= -14)
+	{
+		double m = nearbyint(ldexp(a, 11 - ex));   // 11 significant bits, in [1024, 2048]
+		int e = ex - 1;
+		if (m >= 2048.0) { m = 1024.0; e++; }
+		return (uint16_t)(sign | ((e + 15) << 10) | ((int)m - 1024));
+	}
+	const double q = nearbyint(ldexp(a, 24));     // subnormal: multiples of 2^-24
+	return (uint16_t)(sign | (int)q);              // q == 1024 is the smallest normal's bits
+}
 
 int build_image(const HostGrid& g, unsigned flags, GridImage& im)
 {
@@ -1956,8 +2078,7 @@ int build_image(const HostGrid& g, unsigned flags, GridImage& im)
 				if (L.lo_index[n] != ~0u) im.s64c[(size_t)L.lo_index[n] * im.ld + o] = v;
 			}
 		// row maxima for the FP32C form's negligible-term test: a fine term is
-		// dropped when |w| * max|s_row| < 2^-46 * max|s| (at most ~2,000
-		// dropped terms per point: below 1e-10 of the largest surplus)
+		// dropped when |w| * max|s_row| < 2^-42 * max|s|
 		im.rowmax.assign(nrow, 0.f);
 		double smax = 0.0;
 		for (int n = 0; n < g.nno; n++)
@@ -1967,7 +2088,30 @@ int build_image(const HostGrid& g, unsigned flags, GridImage& im)
 			im.rowmax[n] = (float)(m * (1.0 + 0x1.0p-20));   // rounded up
 			smax = std::max(smax, m);
 		}
-		im.skip_floor = (float)(ldexp(smax, -46));
+		im.skip_floor = (float)(ldexp(smax, -42));
+		// FP16 rows for fine terms whose bound is below 2^-32 * max|s| (each
+		// such term then carries at most 2^-11 of its bound in rounding), on
+		// grids whose passes are all 256 outputs wide (the rows' lane layout)
+		// and whose row maxima keep the weight scaling in range
+		if (im.ld % 256 == 0 && smax >= 0x1p-80 && smax < 0x1p29)
+		{
+			im.f16_floor = (float)ldexp(smax, -32);
+			im.s16.assign(nrow * im.ld, 0u);
+			for (int n = 0; n < g.nno; n++)
+			{
+				if (im.rowmax[n] <= 0.f) continue;
+				int ex = 0;
+				frexp((double)im.rowmax[n], &ex);          // rowmax in [2^(ex-1), 2^ex)
+				const int k = 14 - (ex - 1);
+				const double* src = &g.surplus[(size_t)n * g.TotalDof];
+				uint16_t* dst = &im.s16[(size_t)n * im.ld];
+				for (int o = 0; o < g.TotalDof; o++)
+				{
+					const int b = o >> 8, r = o & 255, v = r >> 7, l = (r & 127) >> 2, e = r & 3;
+					dst[b * 256 + l * 8 + v * 4 + e] = half_bits(ldexp(src[o], k));
+				}
+			}
+		}
 		// descent layout: groups, and per node (plus the roots' virtual
 		// parent at index nno) {first group, group count, rowmax, FP64 copy row}
 		DescentLayout D;
@@ -2030,6 +2174,7 @@ int upload_image(GridImage& im, int device, sgi_grid_t* out)
 	if (!rc) rc = upload((void**)&d->parent, im.parent.data(), im.parent.size() * 4);
 	if (!rc) rc = upload((void**)&d->aux, im.aux.data(), im.aux.size() * 4);
 	if (!rc && im.nno > 0) rc = upload((void**)&d->ctab, im.ctab.data(), im.ctab.size() * 4);
+	if (!rc && !im.s16.empty()) rc = upload((void**)&d->s16, im.s16.data(), im.s16.size() * 2);
 	if (!rc && !im.s64.empty()) rc = upload((void**)&d->s64, im.s64.data(), im.s64.size() * 8);
 	if (!rc && !im.s32.empty())
 	{
@@ -2043,6 +2188,7 @@ int upload_image(GridImage& im, int device, sgi_grid_t* out)
 	if (rc) { free_grid(d); return rc; }
 	d->nlch = im.nlch;
 	d->skip_floor = d->skip_below = im.skip_floor;
+	d->f16_floor = im.f16_floor;
 	d->parent_h = std::move(im.parent_h);
 	d->skip_h = std::move(im.skip_h);
 	d->depth_h = std::move(im.depth_h);
@@ -2064,7 +2210,7 @@ int upload_image(GridImage& im, int device, sgi_grid_t* out)
 // written before it.  Native byte order: a cache is read back on the machine
 // (or an identical one) that wrote it.
 constexpr char CACHE_MAGIC[8] = { 'S', 'G', 'I', 'L', 'A', 'Y', 'O', 'T' };
-constexpr uint32_t CACHE_VERSION = 1;
+constexpr uint32_t CACHE_VERSION = 2;
 
 struct CacheKey
 {
@@ -2161,13 +2307,14 @@ template <class IO, class Image>
 void cache_fields(IO& io, Image& im)
 {
 	io.val(im.dim); io.val(im.nno); io.val(im.TD); io.val(im.ld); io.val(im.nlch); io.val(im.skip_floor);
+	io.val(im.f16_floor);
 	auto& I = im.info;
 	io.val(I.dim); io.val(I.nno); io.val(I.TotalDof); io.val(I.ld); io.val(I.max_comps); io.val(I.tree_depth);
 	io.val(I.tree_roots); io.val(I.multi_delta); io.val(I.ncoarse); io.val(I.comps); io.val(I.device_bytes);
 	io.val(I.coarse_threshold);
 	io.vec(im.rec); io.vec(im.comps); io.vec(im.coarse_index); io.vec(im.aux); io.vec(im.ctab);
 	io.vec(im.grp_a); io.vec(im.grp_b); io.vec(im.ninfo); io.vec(im.parent);
-	io.vec(im.s64); io.vec(im.s64c); io.vec(im.s32); io.vec(im.rowmax);
+	io.vec(im.s64); io.vec(im.s64c); io.vec(im.s32); io.vec(im.rowmax); io.vec(im.s16);
 	io.vec(im.parent_h); io.vec(im.skip_h); io.vec(im.depth_h);
 	io.vec(im.gfirst_h); io.vec(im.gcount_h); io.vec(im.gcmin_h); io.vec(im.gpmax_h);
 }

@@ -290,7 +290,7 @@ class Grid:
 
     def set_surplus_cutoff(self, cutoff):
         """FP32C only: skip terms whose bound |w| * max|surplus row| is below
-        `cutoff` (absolute; <= 0 restores the form's own 2^-46 * max|surplus|).
+        `cutoff` (absolute; <= 0 restores the form's own 2^-42 * max|surplus|).
         Returns the bound in use."""
         eff = ctypes.c_double()
         _check(lib.sgi_grid_set_surplus_cutoff(self._h, float(cutoff), ctypes.byref(eff)))
@@ -360,9 +360,10 @@ def active_count(grid, x, stream=None):
 
 
 def term_classes(grid, x, stream=None):
-    """FP32C terms per point by class: int64 [npts, 3] = (big, fine, dropped)."""
+    """FP32C terms per point by class: int64 [npts, 4] = (big: FP64 row, fine:
+    FP32 row, fine: FP16 row, dropped)."""
     import torch
-    out = torch.empty((x.shape[0], 3), dtype=torch.int64, device=x.device)
+    out = torch.empty((x.shape[0], 4), dtype=torch.int64, device=x.device)
     _check(lib.sgi_term_classes(grid.handle, x.shape[0], x.data_ptr(), out.data_ptr(), _stream_ptr(stream)))
     return out
 

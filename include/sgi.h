@@ -192,8 +192,9 @@ int sgi_grid_cache_valid(const char* path, int nagents, unsigned flags, const ch
  * term (a row with an FP64 copy whose bound reaches coarse_threshold).  Each
  * output then moves from the FP32C result by at most the sum of the bounds of
  * the terms skipped at that point.  cutoff <= 0, the default, keeps the form's
- * own bound of 2^-46 times the largest |surplus|, and so does any cutoff below
- * it.  `effective` (may be NULL) receives the bound in use.  Calls and plans
+ * own bound of 2^-42 times the largest |surplus|, and so does any cutoff below
+ * it.  A cutoff above 2^-32 times the largest |surplus| also leaves no term
+ * to the FP16 rows (see SGI_FP32C).  `effective` (may be NULL) receives the bound in use.  Calls and plans
  * made afterwards use it; plans made before keep theirs.  Not to be called
  * while another thread calls with this grid.  The FP64 form ignores it.
  * Returns SGI_E_INVALID for a grid built without SGI_BUILD_FP32. */
@@ -202,6 +203,15 @@ int sgi_grid_set_surplus_cutoff(sgi_grid_t g, double cutoff, double* effective);
 /* ---------------------------------------------------------- interpolate */
 #define SGI_FP64   0   /* plain FP64: node order and rounding of the gold kernel */
 #define SGI_FP32C  1   /* FP32 products of small terms, FP64 big terms and sums, FP64 final */
+/* SGI_FP32C classes every term of a point by its bound |w| * max|s_row|
+ * against the grid's largest |surplus| smax: big (at least 2^-16 smax, on a
+ * row with an FP64 copy) reads the FP64 row and adds in FP64; fine reads the
+ * FP32 row, multiplies and sums in FP32 and adds the sums to FP64 every eight
+ * terms; fine terms below 2^-32 smax read an FP16 copy of the row instead
+ * (rows scaled by a power of two per row; grids whose rows are a multiple of
+ * 256 outputs wide); terms below 2^-42 smax are dropped.  Per term the
+ * rounding of the row is at most 2^-24 of its bound (FP32), 2^-11 (FP16), and
+ * a dropped term moves an output by at most its bound. */
 
 /* Batched forward over a set of grids sharing dim and TotalDof (a multistate
  * set or a single grid): grid g owns points [pt_offsets[g], pt_offsets[g+1]).
@@ -276,11 +286,12 @@ int sgi_interpolate_noalloc(int ngrids, const sgi_grid_t* grids, const long long
 /* Active-node count A(x) per point (device int64 out[npts]); diagnostics. */
 int sgi_active_count(sgi_grid_t g, long long npts, const double* x, long long* out, void* stream);
 
-/* The FP32C form's terms per point by class (device int64 out[3 * npts]):
- * out[3p] big terms (rows with an FP64 copy whose bound |w| * max|s_row|
- * reaches the coarse threshold: FP64 row reads), out[3p + 1] fine terms (FP32
- * row reads), out[3p + 2] terms dropped unread (bound below the grid's
- * negligible-term bound or surplus cutoff).  Bounds use the full-product
+/* The FP32C form's terms per point by class (device int64 out[4 * npts]):
+ * out[4p] big terms (rows with an FP64 copy whose bound |w| * max|s_row|
+ * reaches the coarse threshold: FP64 row reads), out[4p + 1] fine terms read
+ * from FP32 rows, out[4p + 2] fine terms read from FP16 rows, out[4p + 3]
+ * terms dropped unread (bound below the grid's negligible-term bound or
+ * surplus cutoff).  Bounds use the full-product
  * weight rounded to FP32; the forward kernels build weights incrementally, so
  * a term within rounding of a threshold may fall on the other side there.
  * Diagnostics (the bytes the forward gathers); SGI_E_INVALID for a grid

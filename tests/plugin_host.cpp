@@ -101,7 +101,7 @@ int main(int argc, char** argv)
 	std::vector<double> xb((size_t)n * dim), vb((size_t)n * TD, 0.0);
 	for (int k = 0; k < n; k++)
 	{
-		st[k] = (5 * k + 1) % nstates;
+		st[k] = (3 * k + 1) % nstates;
 		for (int d = 0; d < dim; d++) xb[(size_t)k * dim + d] = std::fmod(x[d] + 0.01 * k, 1.0);
 	}
 	batch(dev, data, n, st.data(), xb.data(), TD, vb.data());

@@ -59,7 +59,7 @@ def test_plugin_load_through_the_cache(cuda, tmp_path):
     cdir = tmp_path / "caches"
     cdir.mkdir()
     for run in range(2):
-        r = subprocess.run([exe, os.path.join(PKG, "lib", "libsgi_b200.so"), plt, "2"] + [repr(v) for v in x],
+        r = subprocess.run([exe, os.path.join(PKG, "lib", "libsgi_b200.so"), plt, "2"] + [repr(float(v)) for v in x],
                            cwd=tmp_path, capture_output=True, text=True, timeout=300,
                            env=dict(os.environ, SGI_LAYOUT_CACHE=str(cdir)))
         assert r.returncode == 0, r.stderr

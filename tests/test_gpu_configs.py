@@ -119,11 +119,11 @@ def test_c2_multistate_subsample_against_oracle(cuda):
         assert e[0] <= FP32C_TOL, (k, e)
 
 
-def _stressed(case):
-    idx, sur = H.HostGrid.adaptive(59, 40_000, 64, seed=71).arrays()
+def _stressed(case, td):
+    idx, sur = H.HostGrid.adaptive(59, 40_000, td, seed=71).arrays()
     sur = sur.copy()
     if case in ("columns", "both"):
-        sur *= np.array([1.0, 1e-3, 1e-6, 1e-9])[np.arange(64) % 4]
+        sur *= np.array([1.0, 1e-3, 1e-6, 1e-9])[np.arange(td) % 4]
     if case in ("zero_root", "both"):
         root = np.flatnonzero((idx == 0).all(axis=1))
         assert len(root) == 1
@@ -131,13 +131,15 @@ def _stressed(case):
     return idx, sur
 
 
+@pytest.mark.parametrize("td", [64, 256])
 @pytest.mark.parametrize("npts", [64, 12_000])
 @pytest.mark.parametrize("case", ["columns", "zero_root", "both"])
-def test_fp32c_per_output_bound_on_stressed_surpluses(cuda, case, npts):
+def test_fp32c_per_output_bound_on_stressed_surpluses(cuda, case, npts, td):
     """Output columns scaled by 1, 1e-3, 1e-6 and 1e-9, and a zero root row, so
     that a point's outputs are small next to the grid's largest surplus.
-    12,000 points take the large-batch kernels, 64 the small-batch ones."""
-    idx, sur = _stressed(case)
+    12,000 points take the large-batch kernels, 64 the small-batch ones; rows
+    of 256 outputs also read FP16 rows for their smallest fine terms."""
+    idx, sur = _stressed(case, td)
     hg = H.HostGrid.from_dense(idx, sur)
     X = H.gen_points(59, npts, kind=2, seed=72)
     g = H.Grid(hg, flags=H.BUILD_FP32)

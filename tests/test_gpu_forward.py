@@ -425,7 +425,7 @@ def test_surplus_cutoff_error_bound(cuda, variant, flags):
         torch.cuda.synchronize()
         plan_base = out_plan.cpu().numpy()
         floor = g.set_surplus_cutoff(0.0)
-        assert floor == pytest.approx(np.abs(surplus).max() * 2.0 ** -46, rel=1e-6)
+        assert floor == pytest.approx(np.abs(surplus).max() * 2.0 ** -42, rel=1e-6)
         assert g.set_surplus_cutoff(floor / 4) == floor
         smax = np.abs(surplus).max()
         bounds = _term_bounds(index, surplus, X)
@@ -515,7 +515,7 @@ def test_small_batch_two_phase_exact(cuda, case):
     assert np.array_equal(_run(g, X), ref)
     assert np.array_equal(_run(g, X[:1]), ref[:1])
     # FP32C: the same kernels add the FP64 rows of the terms FP32C keeps
-    # (dropped: bound below 2^-46 of the largest surplus)
+    # (dropped: bound below 2^-42 of the largest surplus)
     assert O.rel_error(_run(g, X, H.FP32C), ref)[0] <= FP32C_TOL
     assert np.array_equal(H.interpolate_host(g, X), ref)
     x = torch.from_numpy(X).cuda()
@@ -527,23 +527,27 @@ def test_small_batch_two_phase_exact(cuda, case):
     del plan
 
 
-def test_term_classes_partition_the_active_pairs(cuda):
-    """sgi_term_classes: big + fine + dropped = the active count per point; a
+@pytest.mark.parametrize("td", [64, 256])
+def test_term_classes_partition_the_active_pairs(cuda, td):
+    """sgi_term_classes: big + fine (FP32 rows) + fine (FP16 rows) + dropped =
+    the active count per point; FP16 rows exist for 256-output rows only; a
     higher surplus cutoff only moves fine terms to dropped; an FP64-only grid
     is refused."""
     import torch
-    hg = H.HostGrid.adaptive(59, 20000, 64, seed=8)
+    hg = H.HostGrid.adaptive(59, 20000, td, seed=8)
     g = H.Grid(hg, flags=H.BUILD_FP32)
     x = torch.from_numpy(H.gen_points(59, 700, kind=2, seed=9)).cuda()
     cnt = H.active_count(g, x).cpu().numpy()
     c0 = H.term_classes(g, x).cpu().numpy()
     assert np.array_equal(c0.sum(axis=1), cnt)
-    assert c0[:, 0].sum() > 0 and c0[:, 1].sum() > 0 and c0[:, 2].sum() > 0
-    smax = g.set_surplus_cutoff(0.0) * 2.0 ** 46
+    assert c0[:, 0].sum() > 0 and c0[:, 1].sum() > 0 and c0[:, 3].sum() > 0
+    assert (c0[:, 2].sum() > 0) == (td == 256)
+    smax = g.set_surplus_cutoff(0.0) * 2.0 ** 42
     g.set_surplus_cutoff(smax * 2.0 ** -30)
     c1 = H.term_classes(g, x).cpu().numpy()
     g.set_surplus_cutoff(0.0)
     assert np.array_equal(c1[:, 0], c0[:, 0]) and np.array_equal(c1.sum(axis=1), cnt)
-    assert (c1[:, 2] >= c0[:, 2]).all() and c1[:, 2].sum() > c0[:, 2].sum()
+    assert c1[:, 2].sum() == 0          # the cutoff lies above the FP16 rows' bound
+    assert (c1[:, 3] >= c0[:, 3]).all() and c1[:, 3].sum() > c0[:, 3].sum()
     with pytest.raises(H.SgiError):
         H.term_classes(H.Grid(hg), x)

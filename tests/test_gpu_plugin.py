@@ -26,7 +26,7 @@ def test_plugin_host_single_and_multistate(cuda, tmp_path):
     exe = _build_plugin_host(tmp_path)
     (tmp_path / "hddm-solver.cfg").write_text("n_agents 59\npriorityCUDA 2\n")
     x = DOC["x"]
-    r = subprocess.run([exe, os.path.join(PKG, "lib", "libsgi_b200.so"), PLT, "3"] + [repr(v) for v in x],
+    r = subprocess.run([exe, os.path.join(PKG, "lib", "libsgi_b200.so"), PLT, "3"] + [repr(float(v)) for v in x],
                        cwd=tmp_path, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     lines = r.stdout.strip().splitlines()
@@ -55,7 +55,7 @@ def test_plugin_batch_entry_over_states(cuda, tmp_path):
     nstates = 5
     x = np.array(DOC["x"])
     r = subprocess.run([exe, os.path.join(PKG, "lib", "libsgi_b200.so"), ",".join(files), str(nstates)]
-                       + [repr(v) for v in x], cwd=tmp_path, capture_output=True, text=True, timeout=300,
+                       + [repr(float(v)) for v in x], cwd=tmp_path, capture_output=True, text=True, timeout=300,
                        env=dict(os.environ, PLUGIN_HOST_TOTALDOF="118"))
     assert r.returncode == 0, r.stderr
     golds = [O.Gold.read_plt(f, 59) for f in files]
@@ -63,7 +63,7 @@ def test_plugin_batch_entry_over_states(cuda, tmp_path):
     assert len(rows) == 2 * nstates
     for f in rows:
         k, s = int(f[1]), int(f[2])
-        assert s == (5 * k + 1) % nstates
+        assert s == (3 * k + 1) % nstates
         xk = np.mod(x + 0.01 * k, 1.0)
         ref = golds[s % len(files)].interpolate(xk[None])[0]
         assert np.array_equal(np.array([float(v) for v in f[3:]]), ref), (k, s)
