@@ -41,11 +41,11 @@ CHECK_POINTS, CHECK_SEED = 4096, 40
 METRIC = "d=59 points/s: batched FP32+comp vs plain FP64 GPU @<=1e-7 rel err; %HBM peak"
 WORKLOAD = "C4: d=59 adaptive grid, 1M nodes (levels<=7), TotalDof=256, 1M points (half U[0,1], half N(0.5,0.05^2))"
 
-# Random 1 KB surplus-row gathers from an L2-resident region with 16-byte
-# loads, measured on this pool's B200s by a standalone probe: 20.1 TB/s with 64
-# warps per SM, 14.6 TB/s with 32 (four blocks of eight warps, the occupancy
-# of the forward kernels' default variant).
-GATHER_PEAK_TBS = {64: 20.1, 32: 14.6}
+# Random 1 KB surplus-row gathers from an L2-resident region (48 MB) with
+# 16-byte loads, row indices read 32 at a time, measured on this pool's B200s
+# by a standalone probe: 19.7-20.1 TB/s at 24 to 64 warps per SM and one to
+# eight rows in flight per warp (20.2 TB/s for 512-byte rows).
+GATHER_PEAK_TBS = 20.1
 # Warps per SM of the FP32C kernel variants (blocks per SM x 8 warps).
 VARIANT_WARPS = {0: 24, 1: 32, 2: 16}
 
@@ -296,7 +296,7 @@ def run_gpu(args):
         ach = b32 / (ms32 * 1e-3) / 1e9
         gather_b = n_fine * info.ld * 4 + n_half * info.ld * 2 + n_big * info.ld * 8
         warps = VARIANT_WARPS.get(plan32.variant % 3, 32)
-        gpeak = GATHER_PEAK_TBS[64 if warps > 32 else 32]
+        gpeak = GATHER_PEAK_TBS
         gach = gather_b / (ms32 * 1e-3) / 1e12
         sm_mhz = clocks.get("sm_mhz") or 1965.0
         fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
@@ -331,15 +331,14 @@ def run_gpu(args):
                          "traffic_note": "ncu DRAM read+write of one call with the plan's chunking "
                                          "(null when that chunking was not captured)"},
             "gather_roofline": {"bound": "l2_row_gather", "achieved": gach, "unit": "TB/s",
-                                "peak": gpeak, "frac": gach / gpeak, "peak_64_warps_per_sm": GATHER_PEAK_TBS[64],
-                                "frac_of_64_warp_peak": gach / GATHER_PEAK_TBS[64],
+                                "peak": gpeak, "frac": gach / gpeak,
                                 "bytes_per_call": gather_b, "kernel_warps_per_sm": warps,
                                 "terms": {"big_fp64_rows": n_big, "fine_fp32_rows": n_fine,
                                           "fine_fp16_rows": n_half, "dropped": n_drop},
                                 "note": "rows the FP32C kernel reads: fine terms x TotalDof x 4 B (FP32 rows) or "
                                         "x 2 B (FP16 rows) + big terms x TotalDof x 8 B (dropped terms read none), "
-                                        "over the step time; peak: random 1 KB row gathers from L2 at the kernel's "
-                                        "warps per SM"},
+                                        "over the step time; peak: random 1 KB row gathers from an L2-resident "
+                                        "region (standalone probe)"},
             "fma_work": {"active_pairs_per_call": pairs, "flops_per_call": flops,
                          "achieved_tflops": flops / (ms32 * 1e-3) / 1e12,
                          "fp32_peak_tflops": fp32_peak, "frac": flops / (ms32 * 1e-3) / 1e12 / fp32_peak,

@@ -2095,7 +2095,12 @@ int build_image(const HostGrid& g, unsigned flags, GridImage& im)
 		// and whose row maxima keep the weight scaling in range
 		if (im.ld % 256 == 0 && smax >= 0x1p-80 && smax < 0x1p29)
 		{
-			im.f16_floor = (float)ldexp(smax, -32);
+			static const double f16_rel = []()
+			{
+				const char* e = getenv("SGI_F16_REL");
+				return e ? atof(e) : 0x1.0p-32;
+			}();
+			im.f16_floor = (float)(smax * f16_rel);
 			im.s16.assign(nrow * im.ld, 0u);
 			for (int n = 0; n < g.nno; n++)
 			{

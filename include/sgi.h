@@ -209,7 +209,8 @@ int sgi_grid_set_surplus_cutoff(sgi_grid_t g, double cutoff, double* effective);
  * FP32 row, multiplies and sums in FP32 and adds the sums to FP64 every eight
  * terms; fine terms below 2^-32 smax read an FP16 copy of the row instead
  * (rows scaled by a power of two per row; grids whose rows are a multiple of
- * 256 outputs wide); terms below 2^-42 smax are dropped.  Per term the
+ * 256 outputs wide; the environment variable SGI_F16_REL, read once, sets
+ * another fraction of smax); terms below 2^-42 smax are dropped.  Per term the
  * rounding of the row is at most 2^-24 of its bound (FP32), 2^-11 (FP16), and
  * a dropped term moves an output by at most its bound. */
 
