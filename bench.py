@@ -50,12 +50,14 @@ GATHER_PEAK_TBS = 20.1
 VARIANT_WARPS = {0: 24, 1: 32, 2: 16}
 
 # DRAM bytes (read + write) of one FP32C forward call of the default workload,
-# keyed by (node-chunk rows, kernel variant): the sum over the call's
-# fwd_f32d_kernel launches from ncu captures of the same chunking on 65,536
-# and 131,072 points, fitted as a + b * points and taken at 1M points (the
-# per-chunk row reads do not grow with the points; outputs, coordinates and
-# L2 misses do).
-FP32C_CALL_DRAM_BYTES = {}
+# keyed by node-chunk rows: the sum over one call's fwd_f32d_kernel launches
+# in ncu captures of that chunking on 65,536 and 131,072 points (the bench's
+# timed graph replay, --steps 1 --warmup 3), fitted as a + b * points (rows
+# filled into the L2 once per chunk do not grow with the points; carried
+# outputs, coordinates and row misses do), with the kernel variant the
+# captures' plans chose.
+FP32C_CALL_DRAM_BYTES = {97152: {"a": 4.186e8, "b": 70392.0, "variant": 0},
+                         129536: {"a": 2.166e8, "b": 97781.0, "variant": 0}}
 
 
 def env_rank():
@@ -301,7 +303,8 @@ def run_gpu(args):
         sm_mhz = clocks.get("sm_mhz") or 1965.0
         fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
         flops = 2.0 * pairs * TD
-        traffic = FP32C_CALL_DRAM_BYTES.get((plan32.chunk_rows, plan32.variant)) if npts == NPTS else None
+        tfit = FP32C_CALL_DRAM_BYTES.get(plan32.chunk_rows)
+        traffic = tfit["a"] + tfit["b"] * npts if tfit else None
         result = {
             "metric": METRIC,
             "value": pts_s,
@@ -328,8 +331,10 @@ def run_gpu(args):
                          "traffic": traffic, "peak_kind": f"{peak_kind} (burst copy)",
                          "algorithmic_bytes_per_call": b32, "kernel": "fwd_f32d_kernel",
                          "per": f"one forward call: one CUDA-graph replay of {plan32.launches} node-chunk launches",
-                         "traffic_note": "ncu DRAM read+write of one call with the plan's chunking "
-                                         "(null when that chunking was not captured)"},
+                         "traffic_note": "ncu DRAM read+write of one call with the plan's chunking, fitted "
+                                         "over 65,536 and 131,072 points and taken at this run's points "
+                                         "(null when that chunking was not captured)",
+                         "traffic_capture_variant": tfit["variant"] if tfit else None},
             "gather_roofline": {"bound": "l2_row_gather", "achieved": gach, "unit": "TB/s",
                                 "peak": gpeak, "frac": gach / gpeak,
                                 "bytes_per_call": gather_b, "kernel_warps_per_sm": warps,
@@ -366,12 +371,31 @@ def run_gpu(args):
         print(json.dumps(result))
 
 
+def cpu_flags():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def ref_variants():
+    """The reference's SIMD CPU kernels built under oracle/_ref that this host
+    can run and that agree with gold: avx2.  (The reference's avx512 kernel
+    needs the Intel compiler's OpenMP reduction; built without it, it
+    reproduces the reference's fixture but not gold on generated grids.)"""
+    import oracle as O
+    return ["avx2"] if O.ref_available("avx2") and {"avx2", "fma"} <= cpu_flags() else []
+
+
 def cpu_leg(hg, X, o64_sub, o32_sub, sample):
     """Host-side leg (rank 0, one GPU): the oracle checks the timed plans'
     outputs on the 4,096-point subsample (FP64 bit for bit, FP32C relative
-    error), and the reference's own CPU kernel (oracle/_ref, avx2) is timed on
-    a bounded sample of the workload's points, one call per point, all host
-    threads."""
+    error), and the reference's own SIMD CPU kernel (oracle/_ref, avx2) is
+    timed on a bounded sample of the workload's points, one call per point,
+    all host threads."""
     import oracle as O
     cores = os.cpu_count() or 1
     res = {}
@@ -385,27 +409,31 @@ def cpu_leg(hg, X, o64_sub, o32_sub, sample):
             "fp64_max_abs_diff": float(np.abs(o64_sub - ref).max()),
             "fp32c_vs_oracle_gold": {"max_rel_err": emax, "rms_rel_err": erms},
             "note": "outputs of the last timed replay of each plan against the oracle's gold restatement"}
-    variant = "avx2"
-    if not O.ref_available(variant):
+    variants = ref_variants()
+    if not variants:
         res["cpu_baseline"] = {"value": None, "unit": "points/s", "kind": "reference", "cores": 0,
-                               "sample": f"oracle/_ref/libref_{variant}.so not built"}
+                               "sample": "no reference SIMD kernel under oracle/_ref that this host can run"}
         return res
+    half = len(X) // 2
+    pts = np.ascontiguousarray(np.concatenate([X[:sample // 2], X[half:half + sample - sample // 2]]))
+    rates, loads = {}, {}
     with tempfile.TemporaryDirectory() as td:
         p = os.path.join(td, "grid.plt")
         hg.write_plt(p)
-        t = time.time()
-        r = O.RefGrid(p, DIM, variant)
-        t_load = time.time() - t
-        half = len(X) // 2
-        pts = np.ascontiguousarray(np.concatenate([X[:sample // 2], X[half:half + sample - sample // 2]]))
-        r.interpolate(pts[:cores], nthreads=cores)
-        t = time.perf_counter()
-        r.interpolate(pts, nthreads=cores)
-        dt = time.perf_counter() - t
-    res["cpu_baseline"] = {"value": len(pts) / dt, "unit": "points/s", "kind": "reference", "cores": cores,
-                           "variant": variant, "load_s": round(t_load, 1),
+        for variant in variants:
+            t = time.time()
+            r = O.RefGrid(p, DIM, variant)
+            loads[variant] = round(time.time() - t, 1)
+            r.interpolate(pts[:cores], nthreads=cores)
+            t = time.perf_counter()
+            r.interpolate(pts, nthreads=cores)
+            rates[variant] = len(pts) / (time.perf_counter() - t)
+            del r
+    best = max(rates, key=rates.get)
+    res["cpu_baseline"] = {"value": rates[best], "unit": "points/s", "kind": "reference", "cores": cores,
+                           "variant": best, "points_per_s_by_variant": rates, "load_s": loads,
                            "sample": f"{len(pts)} of the workload's points (half uniform, half clustered), "
-                                     f"LinearBasis_{variant}_Generic_InterpolateArray per point, {cores} threads"}
+                                     f"LinearBasis_<variant>_Generic_InterpolateArray per point, {cores} threads"}
     return res
 
 
@@ -418,6 +446,8 @@ def run_reference(args):
         return
     import oracle as O
     variant = args.cpu_variant
+    if variant == "auto":
+        variant = "avx2"
     if not O.ref_available(variant):
         print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/libref_{variant}.so not built "
                           "(needs the reference tree at build time)"}))
@@ -618,7 +648,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=16384,
                     help="points of the CPU baseline's timed sample (default: 16,384)")
     ap.add_argument("--ref-sample", type=int, default=2048, help="--impl reference: points per step")
-    ap.add_argument("--cpu-variant", default="avx2", choices=["gold", "x86", "avx2"])
+    ap.add_argument("--cpu-variant", default="auto", choices=["auto", "gold", "x86", "avx2"],
+                    help="--impl reference: the reference CPU kernel (auto: avx2)")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the host leg (oracle check of the outputs and the CPU baseline)")
     ap.add_argument("--points", type=int, default=NPTS, help="points per GPU (default: the workload's 1M)")

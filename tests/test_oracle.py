@@ -105,3 +105,23 @@ def test_oracle_gradient_matches_finite_differences():
             assert abs(fd - dx[p, k]) <= 1e-5 * max(1.0, abs(fd))
     # dL/dsurplus is linear: sum_p c[p,o] * w_n(x_p)
     assert np.isfinite(ds).all()
+
+
+@pytest.mark.parametrize("variant", ["x86", "avx2"])
+def test_reference_simd_kernels_agree_with_oracle_on_a_generated_grid(tmp_path, variant):
+    """The reference's own sparse CPU kernels (compiled in place) on an
+    adaptive d=59 grid: within 1e-12 of the oracle's gold restatement, which
+    sums in another order."""
+    import bench
+    if not O.ref_available(variant):
+        pytest.skip("reference not compiled here")
+    if variant == "avx2" and not bench.ref_variants():
+        pytest.skip("this host cannot run the avx2 kernel")
+    import hddm_b200 as H
+    hg = H.HostGrid.adaptive(59, 12000, 48, seed=17)
+    p = str(tmp_path / "grid.plt")
+    hg.write_plt(p)
+    X = H.gen_points(59, 300, kind=2, seed=18)
+    ref = O.Gold(*hg.arrays()).interpolate(X)
+    got = O.RefGrid(p, 59, variant).interpolate(X, nthreads=4)
+    assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
