@@ -194,8 +194,9 @@ int sgi_grid_cache_valid(const char* path, int nagents, unsigned flags, const ch
  * the terms skipped at that point.  cutoff <= 0, the default, keeps the form's
  * own bound of 2^-42 times the largest |surplus|, and so does any cutoff below
  * it.  A cutoff above 2^-32 times the largest |surplus| also leaves no term
- * to the FP16 rows (see SGI_FP32C).  `effective` (may be NULL) receives the bound in use.  Calls and plans
- * made afterwards use it; plans made before keep theirs.  Not to be called
+ * to the FP16 rows (see SGI_FP32C).  `effective` (may be NULL) receives the
+ * bound in use.  Calls and plans made afterwards use it; plans made before
+ * keep theirs.  Not to be called
  * while another thread calls with this grid.  The FP64 form ignores it.
  * Returns SGI_E_INVALID for a grid built without SGI_BUILD_FP32. */
 int sgi_grid_set_surplus_cutoff(sgi_grid_t g, double cutoff, double* effective);
