@@ -41,6 +41,14 @@ CHECK_POINTS, CHECK_SEED = 4096, 40
 METRIC = "d=59 points/s: batched FP32+comp vs plain FP64 GPU @<=1e-7 rel err; %HBM peak"
 WORKLOAD = "C4: d=59 adaptive grid, 1M nodes (levels<=7), TotalDof=256, 1M points (half U[0,1], half N(0.5,0.05^2))"
 
+
+def workload_config(npts=NPTS):
+    """The workload as both arms name it (the reference arm times a sample of
+    these points per step and says so in its cpu_baseline)."""
+    return {"workload": WORKLOAD, "dim": DIM, "nno": NNO, "TotalDof": TD, "points_per_gpu": npts,
+            "grid_seed": GRID_SEED, "point_seed": POINT_SEED,
+            "l2": "inputs larger than L2 (x 472 MB, surplus rows 1 GB FP32 / 2 GB FP64)"}
+
 # Random 1 KB surplus-row gathers from an L2-resident region (48 MB) with
 # 16-byte loads, row indices read 32 at a time, measured on this pool's B200s
 # by a standalone probe: 19.7-20.1 TB/s at 24 to 64 warps per SM and one to
@@ -318,11 +326,10 @@ def run_gpu(args):
             "vs_baseline": None,
             "dtype": "f32+comp (f64 in/out)",
             "data": "synthetic: seeded adaptive grid and points (the reference's large grids are not in its tree)",
-            "config": {"workload": WORKLOAD, "dim": DIM, "nno": info.nno, "TotalDof": TD, "points_per_gpu": npts,
-                       "max_comps": info.max_comps, "ncoarse": info.ncoarse, "szxps": szxps,
-                       "mean_active_nodes_per_point": pairs / npts,
-                       "l2": "inputs larger than L2 (x 472 MB, surplus 1 GB FP32 / 2 GB FP64)",
-                       "parallelism": f"replicated grid, points sharded, {world} GPU(s)"},
+            "config": workload_config(npts),
+            "parallelism": f"replicated grid, points sharded, {world} GPU(s)",
+            "workload_stats": {"nno": info.nno, "max_comps": info.max_comps, "ncoarse": info.ncoarse,
+                               "szxps": szxps, "mean_active_nodes_per_point": pairs / npts},
             "points_x_outputs_per_s": pts_s * TD,
             "fp64_form": {"points_per_s": pts64_s, "ms_per_step": ms64,
                           "roofline_frac": b64 / (ms64 * 1e-3) / 1e9 / hbm},
@@ -474,7 +481,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (same grid and points)",
-        "config": {"workload": WORKLOAD, "sample_points_per_step": args.ref_sample},
+        "config": workload_config(),
+        "parallelism": f"host threads over points, {cores} threads",
         "cpu_baseline": {"value": v, "unit": "points/s", "kind": "reference", "cores": cores,
                          "sample": f"{args.ref_sample} random points of the workload per step, "
                                    f"LinearBasis_{variant}_Generic_InterpolateArray, {cores} threads"},
