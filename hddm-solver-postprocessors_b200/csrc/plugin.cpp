@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -16,6 +17,7 @@
 #include <vector>
 
 #include "sgi.h"
+#include "sgi_kernels.h"
 #include "sgi_plugin.h"
 
 // The parent's process facade (include/process.h:8-28), bound weakly.
@@ -386,3 +388,147 @@ extern "C" void sgi_plugin_interpolate_batch(Device* device, Data* data_, int n,
 extern "C" void sgi_plugin_data_free(Data* data) { delete data; }
 
 extern "C" int sgi_plugin_device_index(const Device* device) { return device ? device->index : -1; }
+
+// ------------------------------------------------ kernel-level entry points
+//
+// The reference's x86 kernel signatures over the x86 loader's containers
+// (include/sgi_kernels.h).  The device layout of a container set is built
+// once and kept, keyed on the containers' addresses and sizes and a hash of
+// a sample of their contents.
+
+namespace {
+
+struct X86Key
+{
+	const void* xps;
+	const void* chains;
+	const void* surplus;
+	size_t szxps, nchains;
+	int dim, TD, nno, dimx, ld, nfreqs;
+	uint64_t sample;
+
+	bool operator==(const X86Key& o) const
+	{
+		return xps == o.xps && chains == o.chains && surplus == o.surplus && szxps == o.szxps &&
+		       nchains == o.nchains && dim == o.dim && TD == o.TD && nno == o.nno && dimx == o.dimx &&
+		       ld == o.ld && nfreqs == o.nfreqs && sample == o.sample;
+	}
+};
+
+struct X86Grid
+{
+	X86Key key;
+	int device;
+	sgi_grid_t grid;
+};
+
+std::mutex x86_mtx;
+std::vector<X86Grid> x86_grids;      // most recently built last
+constexpr size_t X86_GRIDS_MAX = 64;
+
+// FNV-1a over at most ~4,096 sampled entries of each container.
+uint64_t x86_sample(const sgi_x86::XPS& xps, const sgi_x86::Chains& chains, const sgi_x86::Matrix<double>& s)
+{
+	uint64_t h = 1469598103934665603ull;
+	auto mix = [&](const void* p, size_t n)
+	{
+		const unsigned char* b = static_cast<const unsigned char*>(p);
+		for (size_t k = 0; k < n; k++) { h ^= b[k]; h *= 1099511628211ull; }
+	};
+	const size_t sx = std::max<size_t>(1, xps.size() / 4096);
+	for (size_t k = 0; k < xps.size(); k += sx) mix(&xps[k], sizeof(xps[k]));
+	const size_t sc = std::max<size_t>(1, chains.size() / 4096);
+	for (size_t k = 0; k < chains.size(); k += sc) mix(&chains[k], sizeof(chains[k]));
+	const size_t ss = std::max<size_t>(1, s.data.size() / 4096);
+	for (size_t k = 0; k < s.data.size(); k += ss) mix(&s.data[k], sizeof(double));
+	return h;
+}
+
+// The grid of one container set on the current device: node n's components
+// from its chain (xps entries up to the first 0), its row of the matrix.
+sgi_grid_t x86_grid(int dim, int DofPerNode, int nfreqs, const sgi_x86::XPS* xps_, const sgi_x86::Chains* chains_,
+	const sgi_x86::Matrix<double>* surplus_)
+{
+	if (!xps_ || !chains_ || !surplus_) die("Null XPS, Chains or surplus\n");
+	const sgi_x86::XPS& xps = *xps_;
+	const sgi_x86::Chains& chains = *chains_;
+	const sgi_x86::Matrix<double>& s = *surplus_;
+	const int nno = s.dimY;
+	if (dim <= 0 || nno < 0 || nfreqs < 0 || DofPerNode <= 0 || DofPerNode > s.dimX ||
+	    s.dimX_aligned < s.dimX || s.data.size() < (size_t)nno * s.dimX_aligned ||
+	    chains.size() < (size_t)nno * nfreqs)
+		die("Inconsistent sparse data: dim %d, nno %d, nfreqs %d, DofPerNode %d, surplus %d x %d\n",
+		    dim, nno, nfreqs, DofPerNode, s.dimY, s.dimX);
+	int dev = 0;
+	cudaGetDevice(&dev);
+	const X86Key key{ xps.data(), chains.data(), s.data.data(), xps.size(), chains.size(), dim, DofPerNode, nno,
+	                  s.dimX, s.dimX_aligned, nfreqs, x86_sample(xps, chains, s) };
+	std::lock_guard<std::mutex> lk(x86_mtx);
+	for (size_t k = 0; k < x86_grids.size(); k++)
+		if (x86_grids[k].device == dev && x86_grids[k].key == key) return x86_grids[k].grid;
+	std::vector<int> index((size_t)nno * 2 * dim, 0);
+	std::vector<double> sur((size_t)nno * DofPerNode);
+	for (int n = 0; n < nno; n++)
+	{
+		for (int f = 0; f < nfreqs; f++)
+		{
+			const uint16_t id = chains[(size_t)n * nfreqs + f];
+			if (!id) break;
+			if (id >= xps.size() || xps[id].index >= dim) die("Chain entry %d of node %d out of range\n", (int)id, n);
+			index[(size_t)n * 2 * dim + xps[id].index] = xps[id].i;
+			index[(size_t)n * 2 * dim + dim + xps[id].index] = xps[id].j;
+		}
+		memcpy(&sur[(size_t)n * DofPerNode], &s.data[(size_t)n * s.dimX_aligned], sizeof(double) * DofPerNode);
+	}
+	sgi_host_grid_t hg = nullptr;
+	if (sgi_host_grid_from_dense(dim, nno, DofPerNode, index.data(), sur.data(), &hg)) die("%s\n", sgi_last_error());
+	sgi_grid_t g = nullptr;
+	const int rc = sgi_grid_create(hg, dev, 0u, &g);
+	sgi_host_grid_free(hg);
+	if (rc) die("%s\n", sgi_last_error());
+	if (x86_grids.size() >= X86_GRIDS_MAX)
+	{
+		sgi_grid_destroy(x86_grids.front().grid);
+		x86_grids.erase(x86_grids.begin());
+	}
+	x86_grids.push_back(X86Grid{ key, dev, g });
+	return g;
+}
+
+} // namespace
+
+// LinearBasis/x86/src/InterpolateArray.cpp:9-54
+extern "C" void LinearBasis_b200_Generic_InterpolateArray(void* device, const int dim, const int DofPerNode,
+	const double* x, const int nfreqs, const sgi_x86::XPS* xps, const sgi_x86::Chains* chains,
+	const sgi_x86::Matrix<double>* surplus, double* value)
+{
+	(void)device;
+	if (!x || !value) die("Null x or value\n");
+	sgi_grid_t g = x86_grid(dim, DofPerNode, nfreqs, xps, chains, surplus);
+	const long long off[2] = { 0, 1 };
+	if (sgi_interpolate_host(1, &g, off, x, value, SGI_FP64)) die("%s\n", sgi_last_error());
+}
+
+// LinearBasis/x86/src/InterpolateArrayManyMultistate.cpp:9-60
+extern "C" void LinearBasis_b200_Generic_InterpolateArrayManyMultistate(void* device, const int dim,
+	const int DofPerNode, const int count, const double* const* x, const int* nfreqs, const sgi_x86::XPS* xps,
+	const sgi_x86::Chains* chains, const sgi_x86::Matrix<double>* surplus, double** value)
+{
+	(void)device;
+	if (count < 0 || (count && (!x || !nfreqs || !xps || !chains || !surplus || !value))) die("Bad multistate call\n");
+	if (!count) return;
+	std::vector<sgi_grid_t> grids(count);
+	std::vector<long long> off(count + 1);
+	std::vector<double> xb((size_t)count * dim), vb((size_t)count * DofPerNode);
+	for (int k = 0; k < count; k++)
+	{
+		grids[k] = x86_grid(dim, DofPerNode, nfreqs[k], &xps[k], &chains[k], &surplus[k]);
+		off[k] = k;
+		if (!x[k] || !value[k]) die("Null x or value of state %d\n", k);
+		memcpy(&xb[(size_t)k * dim], x[k], sizeof(double) * dim);
+	}
+	off[count] = count;
+	if (sgi_interpolate_host(count, grids.data(), off.data(), xb.data(), vb.data(), SGI_FP64))
+		die("%s\n", sgi_last_error());
+	for (int k = 0; k < count; k++) memcpy(value[k], &vb[(size_t)k * DofPerNode], sizeof(double) * DofPerNode);
+}

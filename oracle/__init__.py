@@ -172,6 +172,8 @@ class RefGrid:
             if variant == "x86":
                 L.ref_get_xps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
                 L.ref_get_chains.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+                L.ref_containers.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.POINTER(ctypes.c_int)]
             cls._libs[variant] = L
         return cls._libs[variant]
 
@@ -203,6 +205,14 @@ class RefGrid:
         out = np.zeros((inf["nno"], 2 * inf["dim"]), np.int32)
         self.L.ref_get_index(self.h, istate, out.ctypes.data)
         return out
+
+    def containers(self, istate=0):
+        """x86 only: addresses of the loaded state's XPS, Chains and surplus
+        Matrix objects (valid while this RefGrid lives) and its nfreqs."""
+        out = (ctypes.c_void_p * 3)()
+        nf = ctypes.c_int(0)
+        self.L.ref_containers(self.h, istate, out, ctypes.byref(nf))
+        return out[0], out[1], out[2], nf.value
 
     def xps_chains(self, istate=0):
         inf = self.info(istate)

@@ -216,6 +216,18 @@ void ref_get_chains(void* hv, int istate, int* out)
 	for (size_t k = 0; k < c.size(); k++)
 		out[k] = c[k];
 }
+
+// Addresses of the loaded state's containers, as the reference's test hands
+// them to a kernel symbol (LinearBasis/tests/InterpolateArray/test.cpp:312-313):
+// out[0] XPS*, out[1] Chains*, out[2] Matrix<double>* (surplus); *nfreqs.
+void ref_containers(void* hv, int istate, void** out, int* nfreqs)
+{
+	RefHandle* h = (RefHandle*)hv;
+	out[0] = &RefAccess::xps(*h->data, istate);
+	out[1] = &RefAccess::chains(*h->data, istate);
+	out[2] = &RefAccess::surplus(*h->data, istate);
+	*nfreqs = RefAccess::nfreqs(*h->data, istate);
+}
 #endif
 
 // Interpolate npts points of state `istate`, one reference kernel call per

@@ -13,11 +13,11 @@ LIB = os.path.join(PKG, "lib", "libsgi_b200.so")
 
 def _declared_functions():
     names = set()
-    for h in ("sgi.h", "sgi_plugin.h"):
+    for h in ("sgi.h", "sgi_plugin.h", "sgi_kernels.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         src = re.sub(r"//[^\n]*", "", src)
-        if h == "sgi_plugin.h":
+        if h in ("sgi_plugin.h", "sgi_kernels.h"):
             src = src[src.index('extern "C"'):]
         for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{}]*\)\s*;", src):
             name = m.group(1)
@@ -30,7 +30,9 @@ def test_header_declares_expected_entry_points():
     names = _declared_functions()
     for must in ("sgi_interpolate", "sgi_interpolate_host", "sgi_backward", "sgi_grid_create",
                  "getInterpolator", "getData", "isSupported", "getPriority", "resetInterpolator",
-                 "tryAcquireDevice", "releaseDevice", "getDeviceProperties"):
+                 "tryAcquireDevice", "releaseDevice", "getDeviceProperties",
+                 "LinearBasis_b200_Generic_InterpolateArray",
+                 "LinearBasis_b200_Generic_InterpolateArrayManyMultistate"):
         assert must in names
 
 
