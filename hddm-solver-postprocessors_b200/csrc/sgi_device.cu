@@ -562,7 +562,7 @@ __host__ __device__ __forceinline__ int list_stride(int dim) { return FCAP + WPA
 // of Q rows; their FP32 partial sums are added to the outputs' FP64 running
 // sums every FLUSH terms.  Fine terms below 2^-42 of the largest surplus are
 // dropped before their row is read; in the descent form, fine terms below
-// 2^-32 of it read FP16 copies of their rows (see half_lo_scaled).  The
+// 2^-32 of it read FP16 copies of their rows (see halves_to_float).  The
 // running sums also carry the outputs across node chunks.
 constexpr int FLUSH = 8;
 
@@ -785,20 +785,19 @@ __host__ __device__ __forceinline__ int desc_stride(int dim) { return 2 * SCAP +
 // in [2^14, 2^15).  Within each block of 256 outputs, lane l's 16 bytes hold
 // outputs 128 v + 4 l + e (v = 0, 1; e = 0..3) in that order: the outputs the
 // lane owns in the two-by-four output layout, one 16-byte load per row.
-// Moving a half's bits up by 13 (sign up by 16) gives an FP32 of its value
-// times 2^-112, subnormal halves included; the term's weight is scaled by
-// 2^(112 - k_n) = 2^(98 + floor(log2(rowmax_n))) when it is listed.
-__device__ __forceinline__ float half_lo_scaled(uint32_t u)
+// The halves convert to FP32 exactly (one conversion instruction each,
+// subnormal halves included), and the term's weight is scaled by
+// 2^-k_n = 2^(floor(log2(rowmax_n)) - 14) when it is listed.  The host
+// builds FP16 rows only for grids whose largest |surplus| is at least 2^-60,
+// so that this scale (rowmax_n >= 2^-42 of it for any listed term) and the
+// scaled weight stay normal FP32 numbers.
+__device__ __forceinline__ void halves_to_float(uint32_t u, float& lo, float& hi)
 {
-	return __uint_as_float(((u << 16) & 0x80000000u) | ((u << 13) & 0x0fffe000u));
-}
-__device__ __forceinline__ float half_hi_scaled(uint32_t u)
-{
-	return __uint_as_float((u & 0x80000000u) | ((u >> 3) & 0x0fffe000u));
+	asm("{ .reg .b16 l, h; mov.b32 {l, h}, %2; cvt.f32.f16 %0, l; cvt.f32.f16 %1, h; }" : "=f"(lo), "=f"(hi) : "r"(u));
 }
 __device__ __forceinline__ float f16_weight(float wf, uint32_t rowmax_bits)
 {
-	return wf * __uint_as_float((((rowmax_bits >> 23) & 0xffu) + 98u) << 23);
+	return wf * __uint_as_float((((rowmax_bits >> 23) & 0xffu) - 14u) << 23);
 }
 static_assert(FCAP >= 32, "the chain weights (32 doubles) alias the fine-term list");
 
@@ -921,13 +920,36 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 						for (int v = 0; v < V; v++)
 							load_row<E>(row, v * 32 * E, FULLROW || lcol + v * 32 * E < (int)ld, sv[q][v]);
 					}
+					// two outputs per packed FMA (each output's own rounding
+					// and order, as with one FMA per output)
+					if constexpr (E % 2 == 0)
+					{
 #pragma unroll
-					for (int v = 0; v < V; v++)
+						for (int v = 0; v < V; v++)
 #pragma unroll
-						for (int e = 0; e < E; e++)
+							for (int e = 0; e < E; e += 2)
+							{
+								float2 pp = make_float2(part[v][e], part[v][e + 1]);
 #pragma unroll
-							for (int q = 0; q < Q; q++)
-								part[v][e] = __fmaf_rn(__uint_as_float(en[q].y), sv[q][v][e], part[v][e]);
+								for (int q = 0; q < Q; q++)
+								{
+									const float wq = __uint_as_float(en[q].y);
+									pp = __ffma2_rn(make_float2(wq, wq), make_float2(sv[q][v][e], sv[q][v][e + 1]), pp);
+								}
+								part[v][e] = pp.x;
+								part[v][e + 1] = pp.y;
+							}
+					}
+					else
+					{
+#pragma unroll
+						for (int v = 0; v < V; v++)
+#pragma unroll
+							for (int e = 0; e < E; e++)
+#pragma unroll
+								for (int q = 0; q < Q; q++)
+									part[v][e] = __fmaf_rn(__uint_as_float(en[q].y), sv[q][v][e], part[v][e]);
+					}
 					since += Q;
 					if (since >= FLUSH) { flush(); since = 0; }
 				}
@@ -951,15 +973,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 #pragma unroll
 					for (int q = 0; q < Q16; q++)
 					{
-						const float w = __uint_as_float(en[q].y);
-						part[0][0] = __fmaf_rn(w, half_lo_scaled(hv[q].x), part[0][0]);
-						part[0][1] = __fmaf_rn(w, half_hi_scaled(hv[q].x), part[0][1]);
-						part[0][2] = __fmaf_rn(w, half_lo_scaled(hv[q].y), part[0][2]);
-						part[0][3] = __fmaf_rn(w, half_hi_scaled(hv[q].y), part[0][3]);
-						part[V - 1][0] = __fmaf_rn(w, half_lo_scaled(hv[q].z), part[V - 1][0]);
-						part[V - 1][1] = __fmaf_rn(w, half_hi_scaled(hv[q].z), part[V - 1][1]);
-						part[V - 1][2] = __fmaf_rn(w, half_lo_scaled(hv[q].w), part[V - 1][2]);
-						part[V - 1][3] = __fmaf_rn(w, half_hi_scaled(hv[q].w), part[V - 1][3]);
+						const float2 ww = make_float2(__uint_as_float(en[q].y), __uint_as_float(en[q].y));
+						float f[8];
+						halves_to_float(hv[q].x, f[0], f[1]);
+						halves_to_float(hv[q].y, f[2], f[3]);
+						halves_to_float(hv[q].z, f[4], f[5]);
+						halves_to_float(hv[q].w, f[6], f[7]);
+						float2 pp;
+						pp = __ffma2_rn(ww, make_float2(f[0], f[1]), make_float2(part[0][0], part[0][1]));
+						part[0][0] = pp.x; part[0][1] = pp.y;
+						pp = __ffma2_rn(ww, make_float2(f[2], f[3]), make_float2(part[0][2], part[0][3]));
+						part[0][2] = pp.x; part[0][3] = pp.y;
+						pp = __ffma2_rn(ww, make_float2(f[4], f[5]), make_float2(part[V - 1][0], part[V - 1][1]));
+						part[V - 1][0] = pp.x; part[V - 1][1] = pp.y;
+						pp = __ffma2_rn(ww, make_float2(f[6], f[7]), make_float2(part[V - 1][2], part[V - 1][3]));
+						part[V - 1][2] = pp.x; part[V - 1][3] = pp.y;
 					}
 					since += Q16;
 					if (since >= FLUSH) { flush(); since = 0; }
@@ -2092,8 +2120,8 @@ int build_image(const HostGrid& g, unsigned flags, GridImage& im)
 		// FP16 rows for fine terms whose bound is below 2^-32 * max|s| (each
 		// such term then carries at most 2^-11 of its bound in rounding), on
 		// grids whose passes are all 256 outputs wide (the rows' lane layout)
-		// and whose row maxima keep the weight scaling in range
-		if (im.ld % 256 == 0 && smax >= 0x1p-80 && smax < 0x1p29)
+		// and whose row maxima keep the weight scaling a normal FP32 number
+		if (im.ld % 256 == 0 && smax >= 0x1p-60 && smax < 0x1p100)
 		{
 			static const double f16_rel = []()
 			{
@@ -2215,7 +2243,7 @@ int upload_image(GridImage& im, int device, sgi_grid_t* out)
 // written before it.  Native byte order: a cache is read back on the machine
 // (or an identical one) that wrote it.
 constexpr char CACHE_MAGIC[8] = { 'S', 'G', 'I', 'L', 'A', 'Y', 'O', 'T' };
-constexpr uint32_t CACHE_VERSION = 2;
+constexpr uint32_t CACHE_VERSION = 3;
 
 struct CacheKey
 {
