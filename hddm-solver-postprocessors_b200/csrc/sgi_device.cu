@@ -562,7 +562,7 @@ __host__ __device__ __forceinline__ int list_stride(int dim) { return FCAP + WPA
 // of Q rows; their FP32 partial sums are added to the outputs' FP64 running
 // sums every FLUSH terms.  Fine terms below 2^-42 of the largest surplus are
 // dropped before their row is read; in the descent form, fine terms below
-// 2^-32 of it read FP16 copies of their rows (see halves_to_float).  The
+// 2^-29 of it read FP16 copies of their rows (see halves_to_float).  The
 // running sums also carry the outputs across node chunks.
 constexpr int FLUSH = 8;
 
@@ -1931,7 +1931,7 @@ struct sgi_grid
 	float* rowmax = nullptr;
 	float skip_below = 0.f;      // in use: the larger of skip_floor and the surplus cutoff
 	float skip_floor = 0.f;      // FP32C's own negligible-term bound, 2^-42 of max |surplus|
-	float f16_floor = 0.f;       // FP32C: fine terms below this bound read the FP16 rows (2^-32 of max |surplus|)
+	float f16_floor = 0.f;       // FP32C: fine terms below this bound read the FP16 rows (2^-29 of max |surplus|)
 	uint4* s16 = nullptr;        // FP16 rows (see the kernels' description), or null
 	uint2* aux = nullptr;
 	double* s64 = nullptr;
@@ -2117,8 +2117,10 @@ int build_image(const HostGrid& g, unsigned flags, GridImage& im)
 			smax = std::max(smax, m);
 		}
 		im.skip_floor = (float)(ldexp(smax, -42));
-		// FP16 rows for fine terms whose bound is below 2^-32 * max|s| (each
-		// such term then carries at most 2^-11 of its bound in rounding), on
+		// FP16 rows for fine terms whose bound is below 2^-29 * max|s| (each
+		// such term then carries at most 2^-11 of its bound, below 2^-40 *
+		// max|s|, in rounding: no more than an FP32 row gives the largest fine
+		// terms, 2^-24 of a bound below 2^-16 * max|s|), on
 		// grids whose passes are all 256 outputs wide (the rows' lane layout)
 		// and whose row maxima keep the weight scaling a normal FP32 number
 		if (im.ld % 256 == 0 && smax >= 0x1p-60 && smax < 0x1p100)
@@ -2126,7 +2128,7 @@ int build_image(const HostGrid& g, unsigned flags, GridImage& im)
 			static const double f16_rel = []()
 			{
 				const char* e = getenv("SGI_F16_REL");
-				return e ? atof(e) : 0x1.0p-32;
+				return e ? atof(e) : 0x1.0p-29;
 			}();
 			im.f16_floor = (float)(smax * f16_rel);
 			im.s16.assign(nrow * im.ld, 0u);

@@ -193,7 +193,7 @@ int sgi_grid_cache_valid(const char* path, int nagents, unsigned flags, const ch
  * output then moves from the FP32C result by at most the sum of the bounds of
  * the terms skipped at that point.  cutoff <= 0, the default, keeps the form's
  * own bound of 2^-42 times the largest |surplus|, and so does any cutoff below
- * it.  A cutoff above 2^-32 times the largest |surplus| also leaves no term
+ * it.  A cutoff above 2^-29 times the largest |surplus| also leaves no term
  * to the FP16 rows (see SGI_FP32C).  `effective` (may be NULL) receives the
  * bound in use.  Calls and plans made afterwards use it; plans made before
  * keep theirs.  Not to be called
@@ -208,12 +208,13 @@ int sgi_grid_set_surplus_cutoff(sgi_grid_t g, double cutoff, double* effective);
  * against the grid's largest |surplus| smax: big (at least 2^-16 smax, on a
  * row with an FP64 copy) reads the FP64 row and adds in FP64; fine reads the
  * FP32 row, multiplies and sums in FP32 and adds the sums to FP64 every eight
- * terms; fine terms below 2^-32 smax read an FP16 copy of the row instead
+ * terms; fine terms below 2^-29 smax read an FP16 copy of the row instead
  * (rows scaled by a power of two per row; grids whose rows are a multiple of
  * 256 outputs wide; the environment variable SGI_F16_REL, read once, sets
  * another fraction of smax); terms below 2^-42 smax are dropped.  Per term the
- * rounding of the row is at most 2^-24 of its bound (FP32), 2^-11 (FP16), and
- * a dropped term moves an output by at most its bound. */
+ * rounding of the row is at most 2^-24 of its bound (FP32), 2^-11 (FP16), in
+ * either case below 2^-40 smax, and a dropped term moves an output by at most
+ * its bound. */
 
 /* Batched forward over a set of grids sharing dim and TotalDof (a multistate
  * set or a single grid): grid g owns points [pt_offsets[g], pt_offsets[g+1]).

@@ -543,7 +543,7 @@ def test_term_classes_partition_the_active_pairs(cuda, td):
     assert c0[:, 0].sum() > 0 and c0[:, 1].sum() > 0 and c0[:, 3].sum() > 0
     assert (c0[:, 2].sum() > 0) == (td == 256)
     smax = g.set_surplus_cutoff(0.0) * 2.0 ** 42
-    g.set_surplus_cutoff(smax * 2.0 ** -30)
+    g.set_surplus_cutoff(smax * 2.0 ** -28)
     c1 = H.term_classes(g, x).cpu().numpy()
     g.set_surplus_cutoff(0.0)
     assert np.array_equal(c1[:, 0], c0[:, 0]) and np.array_equal(c1.sum(axis=1), cnt)
