@@ -64,8 +64,8 @@ VARIANT_WARPS = {0: 24, 1: 32, 2: 16}
 # filled into the L2 once per chunk do not grow with the points; carried
 # outputs, coordinates and row misses do), with the kernel variant the
 # captures' plans chose.
-FP32C_CALL_DRAM_BYTES = {97152: {"a": 4.186e8, "b": 70392.0, "variant": 0},
-                         129536: {"a": 2.166e8, "b": 97781.0, "variant": 0}}
+FP32C_CALL_DRAM_BYTES = {97152: {"a": 4.016e8, "b": 60956.0, "variant": "2 at 65,536 points, 1 at 131,072"},
+                         129536: {"a": 2.133e8, "b": 85875.0, "variant": "2 at 65,536 points, 1 at 131,072"}}
 
 
 def env_rank():
