@@ -823,6 +823,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) fwd_f32d_kernel(const __grid_cons
 	// full 256-output passes (the layout of the rows)
 	constexpr bool F16 = V == 2 && E == 4 && FULLROW;
 	constexpr int Q16 = 2 * Q;   // FP16 rows per group: the registers of Q FP32 rows
+	// the final padding fills entries below 32 only: a group size that does not
+	// divide 32 could pad past them and read stale row indices
+	static_assert(32 % Q16 == 0, "groups of Q16 must tile a step's hits");
 	const bool first = a.chunk_begin == 0;
 	for (;;)
 	{
