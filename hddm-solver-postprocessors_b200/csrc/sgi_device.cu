@@ -1754,7 +1754,7 @@ struct DeviceWork
 	// host-pointer staging
 	double* dx = nullptr; size_t dx_bytes = 0;
 	double* dout = nullptr; size_t dout_bytes = 0;
-	cudaStream_t stream = nullptr, copy_in = nullptr, copy_out = nullptr;
+	cudaStream_t stream = nullptr, stream2 = nullptr, copy_in = nullptr, copy_out = nullptr;
 	static constexpr int NEV = 8;
 	cudaEvent_t ev_in[NEV] = {}, ev_done[NEV] = {};
 	// stream-ordered scratch (backward pass, small-batch hit lists): a
@@ -2900,6 +2900,7 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 		CUDA_TRY(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
 		CUDA_TRY(cudaStreamCreateWithFlags(&W->copy_in, cudaStreamNonBlocking));
 		CUDA_TRY(cudaStreamCreateWithFlags(&W->copy_out, cudaStreamNonBlocking));
+		CUDA_TRY(cudaStreamCreateWithFlags(&W->stream2, cudaStreamNonBlocking));
 		for (int k = 0; k < DeviceWork::NEV; k++)
 		{
 			CUDA_TRY(cudaEventCreateWithFlags(&W->ev_in[k], cudaEventDisableTiming));
@@ -2911,21 +2912,25 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 	if (W->dx_bytes < xb) { cudaFree(W->dx); W->dx = nullptr; W->dx_bytes = 0; CUDA_TRY(cudaMalloc(&W->dx, xb)); W->dx_bytes = xb; }
 	if (W->dout_bytes < ob) { cudaFree(W->dout); W->dout = nullptr; W->dout_bytes = 0; CUDA_TRY(cudaMalloc(&W->dout, ob)); W->dout_bytes = ob; }
 	// With pinned host buffers the batch is cut into sub-batches whose copies
-	// in and out overlap the other sub-batches' kernels (three streams); with
+	// in and out overlap the other sub-batches' kernels (a copy stream each
+	// way, and two compute streams that the sub-batches alternate between, so
+	// that one sub-batch's launches fill the tails of the other's); with
 	// pageable buffers the copies would block the host, so it runs as one.
 	cudaPointerAttributes ax{}, ao{};
 	const bool pinned = cudaPointerGetAttributes(&ax, x) == cudaSuccess && ax.type == cudaMemoryTypeHost &&
 		cudaPointerGetAttributes(&ao, out) == cudaSuccess && ao.type == cudaMemoryTypeHost;
 	cudaGetLastError();
-	// sub-batches of about 256k points (at most 8): the first sub-batch's copy
+	// sub-batches of about 128k points (at most 8): the first sub-batch's copy
 	// in and the last one's copy out are all that the kernels do not hide,
-	// while every sub-batch repeats all node-chunk launches and their tails
-	// (on d=59, 1M nodes, TotalDof 256, 1M points: 1, 2, 4, 8, 16 equal
-	// sub-batches took 147, 129, 125, 131, 155 ms).  With three or more, the
-	// first and the last are half the size of the others: their exposed
-	// copies shrink while each middle sub-batch's copy out still fits under
-	// the next one's kernels.
-	const int nsub = !pinned ? 1 : (int)std::min(8ll, std::max(1ll, (npts + 128 * 1024) / (256 * 1024)));
+	// while every sub-batch repeats all node-chunk launches, whose tails the
+	// other compute stream fills (on d=59, 1M nodes, TotalDof 256, 1M
+	// points, FP32C: 2 / 3 / 4 / 6 / 8 sub-batches took 114.9 / 106.2 /
+	// 106.5 / 109.1 / 113.5 ms on one compute stream, 126.7 / 108.8 / 108.9 /
+	// 104.4 / 101.0 ms on two, 102.8 ms for 8 on three; 10, 12 and 16 on two
+	// 102.0, 101.5 and 105.5 ms).  With three or more, the first and the last
+	// are half the size of the others: their exposed copies shrink while each
+	// middle sub-batch's copy out still fits under the next one's kernels.
+	const int nsub = !pinned ? 1 : (int)std::min(8ll, std::max(1ll, (npts + 64 * 1024) / (128 * 1024)));
 	std::vector<long long> cut(nsub + 1);
 	{
 		const long long units = nsub >= 3 ? 2ll * nsub - 2 : nsub;   // weights 1, 2, ..., 2, 1
@@ -2947,7 +2952,8 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 		CUDA_TRY(cudaMemcpyAsync(W->dx + (size_t)P0 * D, x + (size_t)P0 * D, (size_t)(P1 - P0) * D * sizeof(double),
 			cudaMemcpyHostToDevice, W->copy_in));
 		CUDA_TRY(cudaEventRecord(ein, W->copy_in));
-		CUDA_TRY(cudaStreamWaitEvent(W->stream, ein, 0));
+		cudaStream_t cs = (b & 1) ? W->stream2 : W->stream;
+		CUDA_TRY(cudaStreamWaitEvent(cs, ein, 0));
 		// the grids overlapping [P0, P1), offsets relative to P0
 		sg.clear();
 		so.clear();
@@ -2960,15 +2966,16 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 		}
 		so.push_back(P1 - P0);
 		rc = launch_forward((int)sg.size(), sg.data(), so.data(), W->dx + (size_t)P0 * D, W->dout + (size_t)P0 * TD,
-			precision, W->stream);
+			precision, cs);
 		if (rc) return rc;
-		CUDA_TRY(cudaEventRecord(edone, W->stream));
+		CUDA_TRY(cudaEventRecord(edone, cs));
 		CUDA_TRY(cudaStreamWaitEvent(W->copy_out, edone, 0));
 		CUDA_TRY(cudaMemcpyAsync(out + (size_t)P0 * TD, W->dout + (size_t)P0 * TD, (size_t)(P1 - P0) * TD * sizeof(double),
 			cudaMemcpyDeviceToHost, W->copy_out));
 	}
 	CUDA_TRY(cudaStreamSynchronize(W->copy_out));
 	CUDA_TRY(cudaStreamSynchronize(W->stream));
+	CUDA_TRY(cudaStreamSynchronize(W->stream2));
 	return SGI_OK;
 }
 
