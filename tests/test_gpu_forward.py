@@ -316,9 +316,10 @@ def test_wide_component_form_bit_exact(cuda):
 
 
 def test_host_entry_pipelined_sub_batches(cuda):
-    """Pinned host buffers with >= 512k points go through overlapped
-    copy-in / kernel / copy-out sub-batches (here two, the cut inside the
-    first grid's points); FP64 stays gold-exact."""
+    """Pinned host buffers with 192k points or more go through overlapped
+    copy-in / kernel / copy-out sub-batches on two alternating compute
+    streams (here five, of 75k and 150k points, one of them spanning both
+    grids); FP64 stays gold-exact."""
     import ctypes
     import torch
     hosts = [H.HostGrid.adaptive(8, 3000, 40, seed=60), H.HostGrid.adaptive(8, 1500, 40, seed=61)]
