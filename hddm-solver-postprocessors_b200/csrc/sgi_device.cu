@@ -1973,9 +1973,12 @@ int chunk_rows(const DeviceWork* W, const sgi_grid* g0, int precision, long long
 	return (int)rows;
 }
 
+void host_plans_forget(const sgi_grid* g);
+
 void free_grid(sgi_grid* g)
 {
 	if (!g) return;
+	host_plans_forget(g);
 	int prev = 0;
 	cudaGetDevice(&prev);
 	cudaSetDevice(g->device);
@@ -2880,6 +2883,14 @@ extern "C" int sgi_interpolate(int ngrids, const sgi_grid_t* grids, const long l
 	return launch_forward(ngrids, grids, pt_offsets, x, out, precision, (cudaStream_t)stream);
 }
 
+namespace {
+// Host calls of the FP64 form with at most this many points replay a CUDA
+// graph kept per call shape (defined with the plans below).
+constexpr long long HOST_PLAN_MAX_POINTS = 256;
+int host_plan_call(DeviceWork* W, int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, bool* done);
+} // namespace
+
 extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
 	const double* x, double* out, int precision)
 {
@@ -2911,6 +2922,12 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 	const size_t xb = (size_t)npts * D * sizeof(double), ob = (size_t)npts * TD * sizeof(double);
 	if (W->dx_bytes < xb) { cudaFree(W->dx); W->dx = nullptr; W->dx_bytes = 0; CUDA_TRY(cudaMalloc(&W->dx, xb)); W->dx_bytes = xb; }
 	if (W->dout_bytes < ob) { cudaFree(W->dout); W->dout = nullptr; W->dout_bytes = 0; CUDA_TRY(cudaMalloc(&W->dout, ob)); W->dout_bytes = ob; }
+	if (precision == SGI_FP64 && npts <= HOST_PLAN_MAX_POINTS)
+	{
+		bool done = false;
+		rc = host_plan_call(W, ngrids, grids, pt_offsets, x, out, &done);
+		if (rc || done) return rc;
+	}
 	// With pinned host buffers the batch is cut into sub-batches whose copies
 	// in and out overlap the other sub-batches' kernels (a copy stream each
 	// way, and two compute streams that the sub-batches alternate between, so
@@ -3450,3 +3467,120 @@ extern "C" void sgi_plan_destroy(sgi_plan_t p)
 	DeviceGuard guard(p->device);
 	free_plan(p);
 }
+
+namespace {
+
+// Small host calls of the FP64 form (the plugin's one point, or one point per
+// state, per call) replay a plan over the device's staging buffers, kept per
+// call shape (device, grids, point offsets): the call then costs two copies
+// and one graph launch instead of the launches' host set-up.  FP64 results
+// do not depend on the launch configuration, so they are the same bits as
+// the direct launches'.  Entries whose plan would hold more than
+// HOST_PLAN_MAX_SCRATCH of hit-list scratch are not kept; at most
+// HOST_PLANS_MAX shapes per device are, the least recently used replaced
+// first.  An entry goes when one of its grids is destroyed, or when the
+// staging buffers it was recorded on are replaced by larger ones.  Evictions
+// touch only entries of the calling device, whose workspace mutex the
+// caller holds, so no other thread can be replaying them.
+struct HostPlanKey
+{
+	int device;
+	std::vector<const sgi_grid*> grids;
+	std::vector<long long> offs;
+	bool operator<(const HostPlanKey& o) const
+	{
+		return std::tie(device, grids, offs) < std::tie(o.device, o.grids, o.offs);
+	}
+};
+struct HostPlan
+{
+	sgi_plan_t plan;
+	const double* dx;
+	const double* dout;
+	unsigned long long used;
+};
+constexpr size_t HOST_PLANS_MAX = 16;
+constexpr size_t HOST_PLAN_MAX_SCRATCH = 32ull << 20;
+std::mutex g_hp_mtx;
+std::map<HostPlanKey, HostPlan>* g_hp = new std::map<HostPlanKey, HostPlan>();   // kept until exit
+unsigned long long g_hp_clock = 0;
+
+void host_plans_forget(const sgi_grid* g)
+{
+	std::lock_guard<std::mutex> lk(g_hp_mtx);
+	for (auto it = g_hp->begin(); it != g_hp->end();)
+	{
+		if (std::find(it->first.grids.begin(), it->first.grids.end(), g) != it->first.grids.end())
+		{
+			sgi_plan_destroy(it->second.plan);
+			it = g_hp->erase(it);
+		}
+		else ++it;
+	}
+}
+
+int host_plan_call(DeviceWork* W, int ngrids, const sgi_grid_t* grids, const long long* pt_offsets,
+	const double* x, double* out, bool* done)
+{
+	*done = false;
+	const int dev = grids[0]->device;
+	HostPlanKey key{ dev, std::vector<const sgi_grid*>(grids, grids + ngrids),
+	                 std::vector<long long>(pt_offsets, pt_offsets + ngrids + 1) };
+	sgi_plan_t p = nullptr;
+	{
+		std::lock_guard<std::mutex> lk(g_hp_mtx);
+		auto it = g_hp->find(key);
+		if (it != g_hp->end())
+		{
+			if (it->second.dx == W->dx && it->second.dout == W->dout)
+			{
+				p = it->second.plan;
+				it->second.used = ++g_hp_clock;
+			}
+			else
+			{
+				sgi_plan_destroy(it->second.plan);
+				g_hp->erase(it);
+			}
+		}
+	}
+	if (!p)
+	{
+		size_t lb = 0;
+		count_launches(W, ngrids, grids, pt_offsets, SGI_FP64, 0, &lb);
+		if (lb > HOST_PLAN_MAX_SCRATCH) return SGI_OK;            // the direct launches serve
+		if (sgi_plan_create(ngrids, grids, pt_offsets, W->dx, W->dout, SGI_FP64, 0, W->stream, &p) != SGI_OK)
+		{
+			clear_error();
+			return SGI_OK;
+		}
+		std::lock_guard<std::mutex> lk(g_hp_mtx);
+		size_t n = 0;
+		auto lru = g_hp->end();
+		for (auto it = g_hp->begin(); it != g_hp->end(); ++it)
+			if (it->first.device == dev)
+			{
+				n++;
+				if (lru == g_hp->end() || it->second.used < lru->second.used) lru = it;
+			}
+		if (n >= HOST_PLANS_MAX && lru != g_hp->end())
+		{
+			sgi_plan_destroy(lru->second.plan);
+			g_hp->erase(lru);
+		}
+		(*g_hp)[key] = HostPlan{ p, W->dx, W->dout, ++g_hp_clock };
+	}
+	const long long npts = pt_offsets[ngrids];
+	const int D = grids[0]->dim, TD = grids[0]->TD;
+	CUDA_TRY(cudaMemcpyAsync(W->dx, x, (size_t)npts * D * sizeof(double), cudaMemcpyHostToDevice, W->stream));
+	CUDA_TRY(cudaGraphLaunch(p->exec, W->stream));
+	CUDA_TRY(cudaMemcpyAsync(out, W->dout, (size_t)npts * TD * sizeof(double), cudaMemcpyDeviceToHost, W->stream));
+	CUDA_TRY(cudaStreamSynchronize(W->stream));
+	g_stats = sgi_launch_stats{};
+	g_stats.kernels = p->launches;
+	g_stats.points = npts;
+	*done = true;
+	return SGI_OK;
+}
+
+} // namespace
