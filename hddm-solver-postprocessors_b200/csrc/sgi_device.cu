@@ -1961,15 +1961,21 @@ struct sgi_grid
 
 namespace {
 
+// Batches below this many points are not node-chunked by default.
+constexpr long long CHUNK_MIN_POINTS = 81920;
+
 int chunk_rows(const DeviceWork* W, const sgi_grid* g0, int precision, long long npts, int maxnno)
 {
 	const int env = chunk_rows_env();
 	if (env >= 0) return env >= maxnno ? 0 : env;
 	// rows filling half the L2 (the FP32 rows for FP32C): the autotuner's
-	// choice for both forms on the d=59, 1M-node, TotalDof=256 workload
+	// choice for both forms on the d=59, 1M-node, TotalDof=256 workload.
+	// Smaller batches read each chunk's rows too few times to pay for every
+	// point's set-up per chunk (d=59 grids of 300k and 1M nodes: unchunked is
+	// faster up to 64k points, chunked from 96k points up)
 	const long long row = (long long)g0->ld * (precision == SGI_FP64 ? 8 : 4);
 	const long long rows = std::max(1024ll, (long long)W->l2_bytes / 2 / row);
-	if (npts < 4096 || maxnno <= rows) return 0;
+	if (npts < CHUNK_MIN_POINTS || maxnno <= rows) return 0;
 	return (int)rows;
 }
 

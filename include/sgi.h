@@ -266,7 +266,7 @@ int sgi_backward(sgi_grid_t g, long long npts, const double* x, const double* go
  * pt_offsets); FP64 results are bit-identical to it.  It launches every grid
  * whole, never in node chunks (each chunk launch would take one more counter
  * from the fixed array): on grids whose surplus rows exceed the L2, which
- * sgi_interpolate walks in chunks for batches of 4096 points or more, it
+ * sgi_interpolate walks in chunks for batches of 81,920 points or more, it
  * reads rows from HBM instead of the L2 and is slower, and its FP32C results
  * may differ from sgi_interpolate's in the last bits (the order of the FP64
  * additions differs; both stay within the FP32C tolerance).  Small batches
@@ -305,7 +305,7 @@ int sgi_term_classes(sgi_grid_t g, long long npts, const double* x, long long* o
  * surplus rows exceed the L2 is walked in chunks of consecutive nodes (rows
  * filling half the L2: FP64 rows for FP64, FP32 rows for FP32C), every point against one chunk per launch, the outputs
  * carried between chunks in FP64 (the FP64 form keeps gold's order and bits).
- * rows < 0: automatic (the default; batches under 4096 points are not
+ * rows < 0: automatic (the default; batches under 81,920 points are not
  * chunked); 0: never chunk; > 0: chunks of `rows` nodes.  Returns the previous
  * setting.  No reference counterpart. */
 int sgi_set_chunk_rows(int rows);
