@@ -2965,6 +2965,11 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 			cut[b + 1] = npts * acc / units;
 		}
 	}
+	// the node chunks are chosen for the whole batch, so that sub-batches
+	// below the chunking threshold are chunked as the batch would be
+	int maxnno = 0;
+	for (int k = 0; k < ngrids; k++) maxnno = std::max(maxnno, grids[k]->nno);
+	const int chunk = chunk_rows(W, g0, precision, npts, maxnno);
 	std::vector<sgi_grid_t> sg;
 	std::vector<long long> so;
 	for (int b = 0; b < nsub; b++)
@@ -2989,7 +2994,7 @@ extern "C" int sgi_interpolate_host(int ngrids, const sgi_grid_t* grids, const l
 		}
 		so.push_back(P1 - P0);
 		rc = launch_forward((int)sg.size(), sg.data(), so.data(), W->dx + (size_t)P0 * D, W->dout + (size_t)P0 * TD,
-			precision, cs);
+			precision, cs, chunk);
 		if (rc) return rc;
 		CUDA_TRY(cudaEventRecord(edone, cs));
 		CUDA_TRY(cudaStreamWaitEvent(W->copy_out, edone, 0));
